@@ -1,0 +1,85 @@
+"""ctypes binding of libq3b.so (include/q3b.h).
+
+Loading fails loudly: there is no CPU fallback for anything this library does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libq3b.so"
+
+OK = 0
+ERR_INVALID, ERR_CUDA, ERR_STATE, ERR_MEMORY, ERR_LINALG, ERR_INTERNAL = 1, 2, 3, 4, 5, 6
+FP64, MIXED = 0, 1
+
+STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "STATE", 4: "MEMORY", 5: "LINALG",
+                6: "INTERNAL"}
+
+
+class Q3BError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"q3b error {STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+class DavidsonOpts(C.Structure):
+    _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_int),
+                ("basis_expansion_factor", C.c_int), ("occupied_bands", C.c_int),
+                ("precision", C.c_int), ("refine_sweeps", C.c_int),
+                ("mixed_tolerance", C.c_double)]
+
+
+class DavidsonStats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("fp64_iterations", C.c_int),
+                ("h_applications", C.c_int), ("unconverged", C.c_int), ("collapses", C.c_int),
+                ("max_residual_norm", C.c_double), ("seconds", C.c_double)]
+
+
+_vp, _i, _d, _sz = C.c_void_p, C.c_int, C.c_double, C.c_size_t
+
+# name -> (restype, argtypes); every symbol declared in include/q3b.h
+SIGNATURES = {
+    "q3b_context_create": (_i, [_i, _sz, C.POINTER(_vp)]),
+    "q3b_context_destroy": (_i, [_vp]),
+    "q3b_last_error": (C.c_char_p, [_vp]),
+    "q3b_get_stream": (_vp, [_vp]),
+    "q3b_set_stream": (_i, [_vp, _vp]),
+    "q3b_synchronize": (_i, [_vp]),
+    "q3b_device_bytes": (_sz, [_vp]),
+    "q3b_set_potential": (_i, [_vp, _vp, _i, _i, _i]),
+    "q3b_invalidate_potential": (_i, [_vp]),
+    "q3b_potential_valid": (_i, [_vp]),
+    "q3b_prepare_kpoint": (_i, [_vp, _i, _vp, _vp, _vp, _i, _i, _vp, _vp]),
+    "q3b_apply_h": (_i, [_vp, _vp, _vp, _i, _i]),
+    "q3b_apply_h_f32": (_i, [_vp, _vp, _vp, _i]),
+    "q3b_apply_h_host": (_i, [_vp, _vp, _vp, _i, _i]),
+}
+
+_lib = None
+
+
+def load(path: os.PathLike | None = None) -> C.CDLL:
+    """Load libq3b.so once and bind every entry point; raise if anything is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise ImportError(f"{p} is missing: build it with `python -m q3_b200.build`")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)          # AttributeError when a symbol is missing
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def check(ctx, rc: int) -> None:
+    if rc != OK:
+        msg = load().q3b_last_error(ctx)
+        raise Q3BError(rc, msg.decode() if msg else "")

@@ -1,0 +1,150 @@
+"""Host-side mirror of the reference's ``PlanewaveHamiltonianApplicator``.
+
+Same method names, argument meaning and error behaviour as
+``src/layer_4_computation/diagonalizer/planewave/internal/hamiltonian_applicator/init.hpp:28-153``,
+over the C ABI of libq3b.so.  Device vectors are torch tensors on the
+context's GPU (complex128, or complex64 for the FP32 entry); host vectors are
+numpy arrays.  Nothing here computes H|psi> itself.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import FP64, MIXED, check
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class Context:
+    """Owns a q3b_context (device, stream, HBM budget, workspaces)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        rc = self.lib.q3b_context_create(int(device), int(hbm_budget), C.byref(h))
+        if rc != 0:
+            raise _lib.Q3BError(rc, f"cannot create a context on device {device}")
+        self.handle = h.value
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.q3b_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return self.lib.q3b_get_stream(self.handle) or 0
+
+    def set_stream(self, stream_ptr: Optional[int]) -> None:
+        check(self.handle, self.lib.q3b_set_stream(self.handle, stream_ptr))
+
+    def synchronize(self) -> None:
+        check(self.handle, self.lib.q3b_synchronize(self.handle))
+
+    def device_bytes(self) -> int:
+        return int(self.lib.q3b_device_bytes(self.handle))
+
+
+class PlanewaveHamiltonianApplicator:
+    """update_potential / prepare_kpoint / apply_batch over libq3b."""
+
+    def __init__(self, context: Optional[Context] = None, device: int = 0, hbm_budget: int = 0):
+        self.ctx = context if context is not None else Context(device, hbm_budget)
+        self.lib = self.ctx.lib
+        self.h = self.ctx.handle
+        self.npw = 0
+        self.grid = None
+        self._keep = []
+
+    # init.hpp:40
+    def update_potential(self, real_space_potential: np.ndarray, grid) -> None:
+        v = np.ascontiguousarray(real_space_potential, dtype=np.float64)
+        n1, n2, n3 = (int(x) for x in grid)
+        if v.size != n1 * n2 * n3:
+            raise ValueError("potential size does not match the grid")
+        check(self.h, self.lib.q3b_set_potential(self.h, _ptr(v), n1, n2, n3))
+        self.grid = (n1, n2, n3)
+
+    # init.hpp:90, :96
+    def invalidate_smooth_potential_cache(self) -> None:
+        check(self.h, self.lib.q3b_invalidate_potential(self.h))
+
+    def is_smooth_potential_cache_valid(self) -> bool:
+        return bool(self.lib.q3b_potential_valid(self.h))
+
+    def is_gamma_only_current(self) -> bool:       # init.hpp:104; full sphere only
+        return False
+
+    def gamma_origin_is_local_current(self) -> bool:  # init.hpp:115; one GPU
+        return True
+
+    # init.hpp:47-50 + the projector set of the k-point
+    def prepare_kpoint(self, kpoint_index: int, number_of_plane_waves: int,
+                       g_vector_to_grid: np.ndarray, kinetic_energy_squared: np.ndarray,
+                       projectors: Optional[np.ndarray] = None,
+                       atom_proj_offsets: Optional[np.ndarray] = None,
+                       d_blocks: Optional[np.ndarray] = None) -> None:
+        npw = int(number_of_plane_waves)
+        g2g = np.ascontiguousarray(g_vector_to_grid, dtype=np.int32)
+        ke = np.ascontiguousarray(kinetic_energy_squared, dtype=np.float64)
+        if g2g.size != npw or ke.size != npw:
+            raise ValueError("plane-wave arrays do not match number_of_plane_waves")
+        if projectors is None or projectors.shape[1] == 0:
+            check(self.h, self.lib.q3b_prepare_kpoint(self.h, npw, _ptr(g2g), _ptr(ke), None, 0,
+                                                      0, None, None))
+        else:
+            beta = np.asfortranarray(projectors, dtype=np.complex128)
+            offs = np.ascontiguousarray(atom_proj_offsets, dtype=np.int32)
+            dblk = np.ascontiguousarray(d_blocks, dtype=np.float64)
+            if beta.shape[0] != npw:
+                raise ValueError("projector rows do not match number_of_plane_waves")
+            check(self.h, self.lib.q3b_prepare_kpoint(self.h, npw, _ptr(g2g), _ptr(ke),
+                                                      _ptr(beta), beta.shape[1], offs.size - 1,
+                                                      _ptr(offs), _ptr(dblk)))
+        self.npw = npw
+        self.kpoint_index = kpoint_index
+
+    def prepare_system_kpoint(self, system, k: int = 0) -> None:
+        """prepare_kpoint from a q3_b200.synthetic System."""
+        kp = system.kpoints[k]
+        self.prepare_kpoint(k, kp.npw, kp.g_to_grid, kp.ke, kp.beta, kp.atom_proj_offsets,
+                            kp.d_blocks)
+
+    # init.hpp:59-61 -- device vectors
+    def apply_batch(self, input_wavefunctions, output_hamiltonian_wavefunctions,
+                    number_of_vectors: int, precision: int = FP64) -> None:
+        psi, hpsi = input_wavefunctions, output_hamiltonian_wavefunctions
+        n = int(number_of_vectors)
+        import torch  # device memory comes from torch; imported only for device calls
+        if psi.device.type != "cuda" or hpsi.device.type != "cuda":
+            raise ValueError("apply_batch takes device tensors; use apply_batch_host for host arrays")
+        if psi.dtype == torch.complex64:
+            if hpsi.dtype != torch.complex64:
+                raise ValueError("FP32 input needs an FP32 output")
+            rc = self.lib.q3b_apply_h_f32(self.h, psi.data_ptr(), hpsi.data_ptr(), n)
+        elif psi.dtype == torch.complex128 and hpsi.dtype == torch.complex128:
+            rc = self.lib.q3b_apply_h(self.h, psi.data_ptr(), hpsi.data_ptr(), n, int(precision))
+        else:
+            raise ValueError("vectors must be complex128 (or complex64 for the FP32 entry)")
+        check(self.h, rc)
+
+    def apply_batch_host(self, psi: np.ndarray, number_of_vectors: int,
+                         precision: int = FP64) -> np.ndarray:
+        x = np.asfortranarray(psi, dtype=np.complex128)
+        out = np.empty_like(x, order="F")
+        check(self.h, self.lib.q3b_apply_h_host(self.h, _ptr(x), _ptr(out),
+                                                int(number_of_vectors), int(precision)))
+        return out

@@ -1,0 +1,136 @@
+// extern "C" entry points of libq3b (include/q3b.h).  Every call converts
+// exceptions to a status code and keeps the message on the context.
+#include <chrono>
+
+#include "context.cuh"
+#include "q3b.h"
+
+using q3b::Context;
+
+namespace {
+
+template <typename F> int guarded(q3b_context* c, F&& f) {
+    if (!c) return Q3B_ERR_INVALID;
+    try {
+        Q3B_CUDA(cudaSetDevice(c->impl.device));
+        f(c->impl);
+        return Q3B_OK;
+    } catch (const std::exception& e) {
+        return q3b::fail(c, e);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int q3b_context_create(int device, size_t hbm_budget_bytes, q3b_context** out) {
+    if (!out) return Q3B_ERR_INVALID;
+    *out = nullptr;
+    try {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+            cudaGetLastError();
+            return Q3B_ERR_CUDA;
+        }
+        *out = new q3b_context(device, hbm_budget_bytes);
+        return Q3B_OK;
+    } catch (const std::exception&) {
+        return Q3B_ERR_CUDA;
+    }
+}
+
+int q3b_context_destroy(q3b_context* ctx) {
+    if (!ctx) return Q3B_ERR_INVALID;
+    delete ctx;
+    return Q3B_OK;
+}
+
+const char* q3b_last_error(const q3b_context* ctx) {
+    return ctx ? ctx->impl.err.c_str() : "null context";
+}
+
+void* q3b_get_stream(q3b_context* ctx) { return ctx ? static_cast<void*>(ctx->impl.stream) : nullptr; }
+
+int q3b_set_stream(q3b_context* ctx, void* s) {
+    return guarded(ctx, [&](Context& c) {
+        c.stream = s ? static_cast<cudaStream_t>(s) : c.own_stream;
+    });
+}
+
+int q3b_synchronize(q3b_context* ctx) {
+    return guarded(ctx, [&](Context& c) { Q3B_CUDA(cudaStreamSynchronize(c.stream)); });
+}
+
+size_t q3b_device_bytes(const q3b_context* ctx) { return ctx ? ctx->impl.held : 0; }
+
+int q3b_set_potential(q3b_context* ctx, const double* v, int n1, int n2, int n3) {
+    return guarded(ctx, [&](Context& c) { c.set_potential(v, n1, n2, n3); });
+}
+
+int q3b_invalidate_potential(q3b_context* ctx) {
+    return guarded(ctx, [&](Context& c) { c.pot_valid = false; });
+}
+
+int q3b_potential_valid(const q3b_context* ctx) { return ctx && ctx->impl.pot_valid ? 1 : 0; }
+
+int q3b_prepare_kpoint(q3b_context* ctx, int npw, const int32_t* g2g, const double* ke,
+                       const q3b_cplx128* beta, int nproj, int natoms, const int32_t* offs,
+                       const double* dblk) {
+    return guarded(ctx, [&](Context& c) {
+        c.prepare_kpoint(npw, g2g, ke, reinterpret_cast<const double2*>(beta), nproj, natoms, offs,
+                         dblk);
+    });
+}
+
+int q3b_apply_h(q3b_context* ctx, const q3b_cplx128* psi, q3b_cplx128* hpsi, int nvec, int precision) {
+    return guarded(ctx, [&](Context& c) {
+        if (nvec < 0 || (nvec > 0 && (!psi || !hpsi))) throw q3b::Status(Q3B_ERR_INVALID, "bad vectors");
+        const int npw = c.kp.npw;
+        if (precision == Q3B_FP64) {
+            c.apply_h<double>(reinterpret_cast<const double2*>(psi), npw,
+                              reinterpret_cast<double2*>(hpsi), npw, nvec);
+        } else if (precision == Q3B_MIXED) {
+            c.require_ready();
+            const size_t n = (size_t)npw * nvec;
+            c.ws_conv_in.reserve(&c, n * sizeof(float2));
+            c.ws_conv_out.reserve(&c, n * sizeof(float2));
+            q3b::convert<double, float>(c.stream, n, reinterpret_cast<const double2*>(psi),
+                                        c.ws_conv_in.as<float2>());
+            c.apply_h<float>(c.ws_conv_in.as<float2>(), npw, c.ws_conv_out.as<float2>(), npw, nvec);
+            q3b::convert<float, double>(c.stream, n, c.ws_conv_out.as<float2>(),
+                                        reinterpret_cast<double2*>(hpsi));
+        } else {
+            throw q3b::Status(Q3B_ERR_INVALID, "unknown precision");
+        }
+    });
+}
+
+int q3b_apply_h_f32(q3b_context* ctx, const q3b_cplx64* psi, q3b_cplx64* hpsi, int nvec) {
+    return guarded(ctx, [&](Context& c) {
+        if (nvec < 0 || (nvec > 0 && (!psi || !hpsi))) throw q3b::Status(Q3B_ERR_INVALID, "bad vectors");
+        c.apply_h<float>(reinterpret_cast<const float2*>(psi), c.kp.npw,
+                         reinterpret_cast<float2*>(hpsi), c.kp.npw, nvec);
+    });
+}
+
+int q3b_apply_h_host(q3b_context* ctx, const q3b_cplx128* psi, q3b_cplx128* hpsi, int nvec,
+                     int precision) {
+    return guarded(ctx, [&](Context& c) {
+        c.require_ready();
+        if (nvec <= 0) return;
+        if (!psi || !hpsi) throw q3b::Status(Q3B_ERR_INVALID, "bad vectors");
+        const size_t n = (size_t)c.kp.npw * nvec;
+        c.ws_host_io.reserve(&c, 2 * n * sizeof(double2));
+        double2* din = c.ws_host_io.as<double2>();
+        double2* dout = din + n;
+        Q3B_CUDA(cudaMemcpyAsync(din, psi, n * sizeof(double2), cudaMemcpyHostToDevice, c.stream));
+        int rc = q3b_apply_h(ctx, reinterpret_cast<q3b_cplx128*>(din), reinterpret_cast<q3b_cplx128*>(dout),
+                             nvec, precision);
+        if (rc != Q3B_OK) throw q3b::Status(rc, c.err);
+        Q3B_CUDA(cudaMemcpyAsync(hpsi, dout, n * sizeof(double2), cudaMemcpyDeviceToHost, c.stream));
+        Q3B_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+}  // extern "C"

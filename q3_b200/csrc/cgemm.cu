@@ -1,0 +1,224 @@
+// Complex GEMMs on CUDA cores; see cgemm.cuh.
+#include "cgemm.cuh"
+
+namespace q3b {
+namespace {
+
+constexpr int kBM = 64;
+constexpr int kBN = 64;
+constexpr int kThreads = 256;
+
+template <typename R> struct GemmTile;
+template <> struct GemmTile<double> { static constexpr int BK = 8; };
+template <> struct GemmTile<float> { static constexpr int BK = 16; };
+
+// One 64x64 tile of C per block, 4x4 complex outputs per thread.  With
+// kchunk < K the block handles K range [z*kchunk, (z+1)*kchunk) and writes its
+// raw sum to part[z] (ld M); otherwise it applies alpha/beta into C.
+template <typename R, bool CONJ_A>
+__global__ void __launch_bounds__(kThreads)
+cgemm_kernel(int M, int N, int K, cplx_t<R> alpha, const cplx_t<R>* __restrict__ A, long lda,
+             const cplx_t<R>* __restrict__ B, long ldb, cplx_t<R> beta, cplx_t<R>* C, long ldc,
+             int kchunk, cplx_t<R>* part) {
+    using T = cplx_t<R>;
+    constexpr int BK = GemmTile<R>::BK;
+    constexpr int LA = (BK * kBM) / kThreads;  // complex loads per thread, A tile
+    constexpr int LB = (BK * kBN) / kThreads;
+    __shared__ T As[2][BK][kBM + 1];
+    __shared__ T Bs[2][BK][kBN + 1];
+
+    const int tid = threadIdx.x;
+    const int tx = tid % 16, ty = tid / 16;
+    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    const int kbeg = blockIdx.z * kchunk;
+    const int kend = min(K, kbeg + kchunk);
+
+    T acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = czero<T>();
+
+    T ra[LA], rb[LB];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int r = 0; r < LA; ++r) {
+            const int idx = tid + r * kThreads;
+            int k, m;
+            if (CONJ_A) {
+                k = idx % BK;
+                m = idx / BK;
+            } else {
+                m = idx % kBM;
+                k = idx / kBM;
+            }
+            const int gk = k0 + k, gm = m0 + m;
+            T v = czero<T>();
+            if (gk < kend && gm < M) {
+                v = CONJ_A ? conj2(A[gk + (long)gm * lda]) : A[gm + (long)gk * lda];
+            }
+            ra[r] = v;
+        }
+#pragma unroll
+        for (int r = 0; r < LB; ++r) {
+            const int idx = tid + r * kThreads;
+            const int k = idx % BK, n = idx / BK;
+            const int gk = k0 + k, gn = n0 + n;
+            rb[r] = (gk < kend && gn < N) ? B[gk + (long)gn * ldb] : czero<T>();
+        }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+        for (int r = 0; r < LA; ++r) {
+            const int idx = tid + r * kThreads;
+            int k, m;
+            if (CONJ_A) {
+                k = idx % BK;
+                m = idx / BK;
+            } else {
+                m = idx % kBM;
+                k = idx / kBM;
+            }
+            As[buf][k][m] = ra[r];
+        }
+#pragma unroll
+        for (int r = 0; r < LB; ++r) {
+            const int idx = tid + r * kThreads;
+            Bs[buf][idx % BK][idx / BK] = rb[r];
+        }
+    };
+
+    int buf = 0;
+    if (kbeg < kend) {
+        load(kbeg);
+        store(0);
+    }
+    __syncthreads();
+    for (int k0 = kbeg; k0 < kend; k0 += BK) {
+        const bool more = (k0 + BK) < kend;
+        if (more) load(k0 + BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            T a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) cfma(acc[i][j], a[i], b[j]);
+        }
+        if (more) store(buf ^ 1);
+        __syncthreads();
+        buf ^= 1;
+    }
+
+    const bool use_beta = (beta.x != R(0) || beta.y != R(0));
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int gm = m0 + ty + 16 * i;
+        if (gm >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int gn = n0 + tx + 16 * j;
+            if (gn >= N) continue;
+            if (part) {
+                part[(long)blockIdx.z * M * N + (long)gn * M + gm] = acc[i][j];
+            } else {
+                T v = cmul(alpha, acc[i][j]);
+                T* c = C + gm + (long)gn * ldc;
+                if (use_beta) v = v + cmul(beta, *c);
+                *c = v;
+            }
+        }
+    }
+}
+
+// C = alpha * sum_z part[z] + beta * C, the splits summed in index order
+template <typename R>
+__global__ void splitk_reduce(int M, int N, int splits, const cplx_t<R>* __restrict__ part,
+                              cplx_t<R> alpha, cplx_t<R> beta, cplx_t<R>* C, long ldc) {
+    using T = cplx_t<R>;
+    const long total = (long)M * N;
+    const bool use_beta = (beta.x != R(0) || beta.y != R(0));
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long)gridDim.x * blockDim.x) {
+        const int m = static_cast<int>(idx % M);
+        const int n = static_cast<int>(idx / M);
+        T s = splits > 0 ? part[idx] : czero<T>();
+        for (int z = 1; z < splits; ++z) s = s + part[(long)z * total + idx];
+        T v = cmul(alpha, s);
+        T* c = C + m + (long)n * ldc;
+        if (use_beta) v = v + cmul(beta, *c);
+        *c = v;
+    }
+}
+
+template <typename R> int choose_splits(int M, int N, int K) {
+    const int tiles = ceil_div(M, kBM) * ceil_div(N, kBN);
+    const int target = 2 * 148;
+    int s = ceil_div(target, tiles);
+    const int kmax = ceil_div(K, 512);
+    if (s > kmax) s = kmax;
+    if (s < 1) s = 1;
+    if (s > 64) s = 64;
+    return s;
+}
+
+}  // namespace
+
+template <typename R> size_t cgemm_workspace_bytes(int M, int N, int K) {
+    const int s = choose_splits<R>(M, N, K);
+    return s > 1 ? (size_t)s * M * N * sizeof(cplx_t<R>) : 0;
+}
+
+template <typename R>
+void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, cplx_t<R> alpha, const cplx_t<R>* A,
+           long lda, const cplx_t<R>* B, long ldb, cplx_t<R> beta, cplx_t<R>* C, long ldc,
+           const GemmWorkspace& ws) {
+    using T = cplx_t<R>;
+    if (M <= 0 || N <= 0) return;
+    constexpr int BK = GemmTile<R>::BK;
+    if (K <= 0) {
+        // C = beta * C
+        dim3 g(ceil_div((long)M * N, 256));
+        splitk_reduce<R><<<g, 256, 0, st>>>(M, N, 0, nullptr, alpha, beta, C, ldc);
+        Q3B_LAUNCH_CHECK();
+        return;
+    }
+    int splits = conj_a ? choose_splits<R>(M, N, K) : 1;
+    size_t need = (size_t)splits * M * N * sizeof(T);
+    if (splits > 1 && (ws.ptr == nullptr || ws.bytes < need)) splits = 1;
+    int kchunk = K;
+    if (splits > 1) {
+        kchunk = ceil_div(K, splits);
+        kchunk = ceil_div(kchunk, BK) * BK;
+        splits = ceil_div(K, kchunk);
+    }
+    dim3 grid(ceil_div(M, kBM), ceil_div(N, kBN), splits);
+    T* part = splits > 1 ? static_cast<T*>(ws.ptr) : nullptr;
+    if (conj_a)
+        cgemm_kernel<R, true><<<grid, kThreads, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                                         ldc, kchunk, part);
+    else
+        cgemm_kernel<R, false><<<grid, kThreads, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
+                                                          ldc, kchunk, part);
+    Q3B_LAUNCH_CHECK();
+    if (splits > 1) {
+        const long total = (long)M * N;
+        int blocks = ceil_div(total, 256);
+        if (blocks > 4096) blocks = 4096;
+        splitk_reduce<R><<<blocks, 256, 0, st>>>(M, N, splits, part, alpha, beta, C, ldc);
+        Q3B_LAUNCH_CHECK();
+    }
+}
+
+template void cgemm<double>(cudaStream_t, bool, int, int, int, double2, const double2*, long,
+                            const double2*, long, double2, double2*, long, const GemmWorkspace&);
+template void cgemm<float>(cudaStream_t, bool, int, int, int, float2, const float2*, long,
+                           const float2*, long, float2, float2*, long, const GemmWorkspace&);
+template size_t cgemm_workspace_bytes<double>(int, int, int);
+template size_t cgemm_workspace_bytes<float>(int, int, int);
+
+}  // namespace q3b

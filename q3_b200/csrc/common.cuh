@@ -1,0 +1,82 @@
+// Shared helpers for the q3b sm_100a kernels: complex arithmetic on float2 /
+// double2, error plumbing, launch checks.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+namespace q3b {
+
+template <typename R> struct CplxOf;
+template <> struct CplxOf<double> { using T = double2; };
+template <> struct CplxOf<float> { using T = float2; };
+template <typename R> using cplx_t = typename CplxOf<R>::T;
+
+__host__ __device__ __forceinline__ double2 mk(double x, double y) { return make_double2(x, y); }
+__host__ __device__ __forceinline__ float2 mk(float x, float y) { return make_float2(x, y); }
+
+__host__ __device__ __forceinline__ double2 operator+(double2 a, double2 b) { return mk(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 operator-(double2 a, double2 b) { return mk(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 operator*(double s, double2 a) { return mk(s * a.x, s * a.y); }
+__host__ __device__ __forceinline__ float2 operator+(float2 a, float2 b) { return mk(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return mk(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 operator*(float s, float2 a) { return mk(s * a.x, s * a.y); }
+
+// complex product a*b
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return mk(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return mk(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// conj(a)*b
+__host__ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
+    return mk(fma(a.x, b.x, a.y * b.y), fma(a.x, b.y, -a.y * b.x));
+}
+__host__ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+    return mk(fmaf(a.x, b.x, a.y * b.y), fmaf(a.x, b.y, -a.y * b.x));
+}
+__host__ __device__ __forceinline__ double2 conj2(double2 a) { return mk(a.x, -a.y); }
+__host__ __device__ __forceinline__ float2 conj2(float2 a) { return mk(a.x, -a.y); }
+// i*a
+__host__ __device__ __forceinline__ double2 mul_i(double2 a) { return mk(-a.y, a.x); }
+__host__ __device__ __forceinline__ float2 mul_i(float2 a) { return mk(-a.y, a.x); }
+
+// acc += a*b
+__device__ __forceinline__ void cfma(double2& acc, double2 a, double2 b) {
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
+}
+__device__ __forceinline__ void cfma(float2& acc, float2 a, float2 b) {
+    acc.x = fmaf(a.x, b.x, acc.x);
+    acc.x = fmaf(-a.y, b.y, acc.x);
+    acc.y = fmaf(a.x, b.y, acc.y);
+    acc.y = fmaf(a.y, b.x, acc.y);
+}
+
+template <typename T> __host__ __device__ __forceinline__ T czero();
+template <> __host__ __device__ __forceinline__ double2 czero<double2>() { return mk(0.0, 0.0); }
+template <> __host__ __device__ __forceinline__ float2 czero<float2>() { return mk(0.0f, 0.0f); }
+
+struct CudaError : std::runtime_error {
+    explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+
+#define Q3B_CUDA(call)                                                                         \
+    do {                                                                                       \
+        cudaError_t q3b_err_ = (call);                                                         \
+        if (q3b_err_ != cudaSuccess) {                                                         \
+            throw ::q3b::CudaError(std::string(#call) + ": " + cudaGetErrorString(q3b_err_)); \
+        }                                                                                      \
+    } while (0)
+
+#define Q3B_LAUNCH_CHECK() Q3B_CUDA(cudaGetLastError())
+
+inline int ceil_div(long a, long b) { return static_cast<int>((a + b - 1) / b); }
+
+}  // namespace q3b

@@ -1,0 +1,345 @@
+// q3b context: HBM accounting, potential, k-point plan, H|psi> orchestration.
+#include <cmath>
+#include <cstring>
+
+#include "context.cuh"
+#include "q3b.h"
+
+namespace q3b {
+
+// ------------------------------------------------------------------ DevBuf
+DevBuf::~DevBuf() { release(); }
+
+void DevBuf::release() {
+    if (ptr) {
+        cudaFree(ptr);
+        if (ctx) ctx->held -= bytes;
+    }
+    ptr = nullptr;
+    bytes = 0;
+}
+
+void DevBuf::reserve(Context* c, size_t need) {
+    if (need <= bytes && ptr) return;
+    release();
+    ctx = c;
+    if (need == 0) return;
+    if (c->budget && c->held + need > c->budget) {
+        throw Status(Q3B_ERR_MEMORY, "HBM budget exceeded: need " + std::to_string(need) +
+                                         " bytes, hold " + std::to_string(c->held) + " of " +
+                                         std::to_string(c->budget));
+    }
+    cudaError_t e = cudaMalloc(&ptr, need);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        cudaGetLastError();
+        throw Status(Q3B_ERR_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    bytes = need;
+    c->held += need;
+}
+
+template <typename T>
+static void upload(Context* c, DevBuf& b, const T* host, size_t count) {
+    b.reserve(c, count * sizeof(T));
+    if (count) Q3B_CUDA(cudaMemcpyAsync(b.ptr, host, count * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+}
+
+// ----------------------------------------------------------------- Context
+Context::Context(int dev, size_t hbm_budget) : device(dev), budget(hbm_budget) {
+    Q3B_CUDA(cudaSetDevice(dev));
+    Q3B_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+    stream = own_stream;
+}
+
+Context::~Context() {
+    // the device buffers are freed by their own destructors after this body
+    cudaSetDevice(device);
+    cudaStreamSynchronize(stream);
+    if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+GemmWorkspace Context::gemm_ws(size_t need) {
+    ws_gemm.reserve(this, need);
+    return GemmWorkspace{ws_gemm.ptr, ws_gemm.bytes};
+}
+
+void Context::require_ready() const {
+    if (!pot_valid) throw Status(Q3B_ERR_STATE, "no valid potential: call q3b_set_potential");
+    if (!kp.valid) throw Status(Q3B_ERR_STATE, "no prepared k-point: call q3b_prepare_kpoint");
+}
+
+void Context::set_potential(const double* v, int a, int b, int c) {
+    if (a <= 0 || b <= 0 || c <= 0 || !v) throw Status(Q3B_ERR_INVALID, "bad potential grid");
+    const bool regrid = (a != n1 || b != n2 || c != n3);
+    n1 = a;
+    n2 = b;
+    n3 = c;
+    const size_t N = (size_t)a * b * c;
+    v_host.assign(v, v + N);
+    std::vector<double> vp(N);
+    std::vector<float> vp32(N);
+    const double inv = 1.0 / static_cast<double>(N);
+    for (int w1 = 0; w1 < a; ++w1)
+        for (int w2 = 0; w2 < b; ++w2)
+            for (int w3 = 0; w3 < c; ++w3) {
+                const double s = v[((size_t)w1 * b + w2) * c + w3] * inv;
+                const size_t d = ((size_t)w3 * a + w1) * b + w2;
+                vp[d] = s;
+                vp32[d] = static_cast<float>(s);
+            }
+    upload(this, v64, vp.data(), N);
+    upload(this, v32, vp32.data(), N);
+    Q3B_CUDA(cudaStreamSynchronize(stream));
+    pot_valid = true;
+    if (regrid && kp.valid) {
+        try {
+            build_plan();
+        } catch (...) {
+            kp.valid = false;  // the k-point must be prepared again on a usable grid
+            throw;
+        }
+    }
+    kp.lp64.vplane = v64.as<double>();
+    kp.lp32.vplane = v32.as<float>();
+}
+
+static void factor_line(int n, int& na, int& nb) {
+    static const int small[] = {1, 2, 3, 4, 5, 6, 8, 9, 10, 12, 15, 16};
+    na = nb = -1;
+    for (int a : small)
+        for (int b : small)
+            if (a * b == n && a >= b && (na < 0 || a < na)) {
+                na = a;
+                nb = b;
+            }
+    if (na < 0) {
+        throw Status(Q3B_ERR_INVALID,
+                     "FFT length " + std::to_string(n) +
+                         " is not a product of two factors from {2,3,4,5,6,8,9,10,12,15,16}");
+    }
+}
+
+template <typename T, typename R> static std::vector<T> twiddles(int n) {
+    std::vector<T> t(n);
+    for (int m = 0; m < n; ++m) {
+        const long double ang = -2.0L * 3.14159265358979323846264338327950288L * m / n;
+        t[m].x = static_cast<R>(cosl(ang));
+        t[m].y = static_cast<R>(sinl(ang));
+    }
+    return t;
+}
+
+void Context::build_plan() {
+    KPoint& k = kp;
+    const long N = (long)n1 * n2 * n3;
+    const int p2 = (n2 % 2 == 0) ? n2 + 1 : n2;
+    const int p3 = (n3 % 2 == 0) ? n3 + 1 : n3;
+    std::vector<int> col_id((size_t)n1 * n2, -1);
+    std::vector<int> unm;
+    std::vector<int> gw1(k.npw), gw2(k.npw), gw3(k.npw), gcol(k.npw, -1);
+    for (int g = 0; g < k.npw; ++g) {
+        const long f = k.g_to_grid[g];
+        if (f < 0 || f >= N) {
+            unm.push_back(g);
+            continue;
+        }
+        const int w1 = static_cast<int>(f / ((long)n2 * n3));
+        const int w2 = static_cast<int>((f / n3) % n2);
+        const int w3 = static_cast<int>(f % n3);
+        gw1[g] = w1;
+        gw2[g] = w2;
+        gw3[g] = w3;
+        gcol[g] = w1 * n2 + w2;
+        col_id[gcol[g]] = 0;
+    }
+    int S = 0;
+    std::vector<int> stick_pos, rows;
+    int last_row = -1;
+    for (int col = 0; col < n1 * n2; ++col) {
+        if (col_id[col] < 0) continue;
+        col_id[col] = S++;
+        const int w1 = col / n2, w2 = col % n2;
+        stick_pos.push_back(w1 * p2 + w2);
+        if (w1 != last_row) {
+            rows.push_back(w1 * p2);
+            last_row = w1;
+        }
+    }
+    std::vector<int> start(S + 1, 0);
+    for (int g = 0; g < k.npw; ++g)
+        if (gcol[g] >= 0) start[col_id[gcol[g]] + 1]++;
+    for (int s = 0; s < S; ++s) start[s + 1] += start[s];
+    const int nent = start[S];
+    std::vector<int> eg(nent), ew3(nent), es(nent), fill(start.begin(), start.end() - 1);
+    for (int g = 0; g < k.npw; ++g) {
+        if (gcol[g] < 0) continue;
+        const int s = col_id[gcol[g]];
+        const int e = fill[s]++;
+        eg[e] = g;
+        ew3[e] = gw3[g];
+        es[e] = s;
+    }
+    upload(this, k.stick_start, start.data(), start.size());
+    upload(this, k.entry_g, eg.data(), eg.size());
+    upload(this, k.entry_w3, ew3.data(), ew3.size());
+    upload(this, k.entry_stick, es.data(), es.size());
+    upload(this, k.stick_pos, stick_pos.data(), stick_pos.size());
+    upload(this, k.row_base, rows.data(), rows.size());
+    upload(this, k.unmapped, unm.data(), unm.size());
+    const int dims[3] = {n1, n2, n3};
+    for (int d = 0; d < 3; ++d) {
+        auto t64 = twiddles<double2, double>(dims[d]);
+        auto t32 = twiddles<float2, float>(dims[d]);
+        upload(this, k.tw64[d], t64.data(), t64.size());
+        upload(this, k.tw32[d], t32.data(), t32.size());
+    }
+    int f[6];
+    factor_line(n1, f[0], f[1]);
+    factor_line(n2, f[2], f[3]);
+    factor_line(n3, f[4], f[5]);
+    auto fillp = [&](auto& lp, const DevBuf* tw, const DevBuf& ke, const DevBuf& vv) {
+        using RR = std::remove_reference_t<decltype(*lp.ke)>;
+        using TT = cplx_t<std::remove_const_t<RR>>;
+        lp.n1 = n1;
+        lp.n2 = n2;
+        lp.n3 = n3;
+        lp.npw = k.npw;
+        lp.nsticks = S;
+        lp.nrows = static_cast<int>(rows.size());
+        lp.p2 = p2;
+        lp.p3 = p3;
+        lp.na1 = f[0];
+        lp.nb1 = f[1];
+        lp.na2 = f[2];
+        lp.nb2 = f[3];
+        lp.na3 = f[4];
+        lp.nb3 = f[5];
+        lp.sg = 32;
+        lp.nunmapped = static_cast<int>(unm.size());
+        lp.stick_start = k.stick_start.as<int>();
+        lp.entry_g = k.entry_g.as<int>();
+        lp.entry_w3 = k.entry_w3.as<int>();
+        lp.entry_stick = k.entry_stick.as<int>();
+        lp.stick_pos = k.stick_pos.as<int>();
+        lp.row_base = k.row_base.as<int>();
+        lp.unmapped_g = k.unmapped.as<int>();
+        lp.tw1 = tw[0].as<TT>();
+        lp.tw2 = tw[1].as<TT>();
+        lp.tw3 = tw[2].as<TT>();
+        lp.ke = ke.as<std::remove_const_t<RR>>();
+        lp.vplane = vv.as<std::remove_const_t<RR>>();
+    };
+    fillp(k.lp64, k.tw64, k.ke64, v64);
+    fillp(k.lp32, k.tw32, k.ke32, v32);
+    if (plane_smem_bytes(k.lp64) > 227 * 1024) {
+        throw Status(Q3B_ERR_INVALID, "FFT plane " + std::to_string(n1) + "x" + std::to_string(n2) +
+                                          " does not fit in shared memory in FP64");
+    }
+    Q3B_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Context::prepare_kpoint(int npw, const int32_t* g2g, const double* ke, const double2* beta,
+                             int nproj, int natoms, const int32_t* offs, const double* dblk) {
+    if (!pot_valid && n1 == 0) throw Status(Q3B_ERR_STATE, "call q3b_set_potential before q3b_prepare_kpoint");
+    if (npw <= 0 || !g2g || !ke) throw Status(Q3B_ERR_INVALID, "bad plane-wave list");
+    if (nproj < 0 || (nproj > 0 && (!beta || natoms <= 0 || !offs || !dblk)))
+        throw Status(Q3B_ERR_INVALID, "bad projector set");
+    kp.valid = false;
+    kp.npw = npw;
+    kp.nproj = nproj;
+    kp.natoms = natoms;
+    kp.g_to_grid.assign(g2g, g2g + npw);
+    kp.ke_host.assign(ke, ke + npw);
+    std::vector<float> ke32(ke, ke + npw);
+    upload(this, kp.ke64, ke, npw);
+    upload(this, kp.ke32, ke32.data(), npw);
+    if (nproj > 0) {
+        if (offs[0] != 0 || offs[natoms] != nproj) throw Status(Q3B_ERR_INVALID, "atom offsets do not cover the projectors");
+        const size_t nb = (size_t)npw * nproj;
+        upload(this, kp.beta64, beta, nb);
+        std::vector<float2> b32(nb);
+        for (size_t i = 0; i < nb; ++i) b32[i] = make_float2((float)beta[i].x, (float)beta[i].y);
+        upload(this, kp.beta32, b32.data(), nb);
+        std::vector<int> ps(nproj), pz(nproj), po(nproj);
+        std::vector<double> d64;
+        size_t doff = 0;
+        for (int a = 0; a < natoms; ++a) {
+            const int s = offs[a], m = offs[a + 1] - offs[a];
+            if (m < 0) throw Status(Q3B_ERR_INVALID, "atom offsets must be non-decreasing");
+            for (int r = 0; r < m; ++r) {
+                ps[s + r] = s;
+                pz[s + r] = m;
+                po[s + r] = static_cast<int>(doff);
+            }
+            for (int i = 0; i < m * m; ++i) {
+                const double d = dblk[doff + i];
+                d64.push_back(std::fabs(d) > 1e-15 ? d : 0.0);
+            }
+            doff += (size_t)m * m;
+        }
+        std::vector<float> d32(d64.begin(), d64.end());
+        upload(this, kp.pstart, ps.data(), ps.size());
+        upload(this, kp.psize, pz.data(), pz.size());
+        upload(this, kp.poff, po.data(), po.size());
+        upload(this, kp.dpk64, d64.data(), d64.size());
+        upload(this, kp.dpk32, d32.data(), d32.size());
+    }
+    build_plan();
+    kp.valid = true;
+}
+
+template <> const LocalPlan<double>& Context::local_plan<double>() const { return kp.lp64; }
+template <> const LocalPlan<float>& Context::local_plan<float>() const { return kp.lp32; }
+
+template <> NonlocalData<double> Context::nonlocal<double>() const {
+    return NonlocalData<double>{kp.nproj, kp.beta64.as<double2>(), kp.pstart.as<int>(),
+                                kp.psize.as<int>(), kp.poff.as<int>(), kp.dpk64.as<double>()};
+}
+template <> NonlocalData<float> Context::nonlocal<float>() const {
+    return NonlocalData<float>{kp.nproj, kp.beta32.as<float2>(), kp.pstart.as<int>(),
+                               kp.psize.as<int>(), kp.poff.as<int>(), kp.dpk32.as<float>()};
+}
+
+template <typename R> int Context::sticks_chunk(int nvec) const {
+    const size_t per = sticks_bytes_per_band(local_plan<R>());
+    const size_t target = 48ull << 20;  // keep a chunk's sticks resident in L2
+    long c = per ? static_cast<long>(target / per) : nvec;
+    if (c < 1) c = 1;
+    if (c > nvec) c = nvec;
+    return static_cast<int>(c);
+}
+
+template <typename R>
+void Context::apply_h(const cplx_t<R>* psi, long ldpsi, cplx_t<R>* hpsi, long ldh, int nvec) {
+    using T = cplx_t<R>;
+    require_ready();
+    if (nvec <= 0) return;
+    const LocalPlan<R>& lp = local_plan<R>();
+    const int chunk = sticks_chunk<R>(nvec);
+    ws_sticks.reserve(this, (size_t)chunk * sticks_bytes_per_band(lp));
+    apply_local<R>(stream, lp, psi, ldpsi, hpsi, ldh, nvec, ws_sticks.as<T>(), chunk);
+    if (kp.nproj > 0) {
+        const size_t pb = (size_t)kp.nproj * nvec * sizeof(T);
+        ws_bm.reserve(this, pb);
+        ws_bp.reserve(this, pb);
+        GemmWorkspace ws = gemm_ws(cgemm_workspace_bytes<R>(kp.nproj, nvec, kp.npw));
+        apply_nonlocal<R>(stream, nonlocal<R>(), kp.npw, nvec, psi, ldpsi, hpsi, ldh,
+                          ws_bm.as<T>(), ws_bp.as<T>(), ws);
+    }
+}
+
+template void Context::apply_h<double>(const double2*, long, double2*, long, int);
+template void Context::apply_h<float>(const float2*, long, float2*, long, int);
+template int Context::sticks_chunk<double>(int) const;
+template int Context::sticks_chunk<float>(int) const;
+
+int fail(q3b_context* c, const std::exception& e) {
+    int code = Q3B_ERR_INTERNAL;
+    if (auto s = dynamic_cast<const Status*>(&e)) code = s->code;
+    else if (dynamic_cast<const CudaError*>(&e)) code = Q3B_ERR_CUDA;
+    if (c) c->impl.err = e.what();
+    return code;
+}
+
+}  // namespace q3b

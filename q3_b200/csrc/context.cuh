@@ -1,0 +1,106 @@
+// The state behind a q3b_context: device, stream, HBM accounting, the
+// potential, the prepared k-point (plane-wave list, sticks plan, projectors)
+// and grow-only workspaces.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "cgemm.cuh"
+#include "common.cuh"
+#include "hpsi_local.cuh"
+#include "nonlocal.cuh"
+
+struct q3b_context;
+
+namespace q3b {
+
+struct Status : std::runtime_error {
+    int code;
+    Status(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+class Context;
+
+// A device allocation charged to its context's HBM budget.
+struct DevBuf {
+    Context* ctx = nullptr;
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf();
+    void release();
+    // grow to at least `need` bytes (contents are not kept)
+    void reserve(Context* c, size_t need);
+    template <typename T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+struct KPoint {
+    int npw = 0;
+    int nproj = 0;
+    int natoms = 0;
+    bool valid = false;
+    std::vector<int> g_to_grid;     // host copy, for replanning on a new grid
+    std::vector<double> ke_host;
+    DevBuf ke64, ke32;
+    DevBuf beta64, beta32;
+    DevBuf pstart, psize, poff, dpk64, dpk32;
+    // sticks plan
+    DevBuf stick_start, entry_g, entry_w3, entry_stick, stick_pos, row_base, unmapped;
+    DevBuf tw64[3], tw32[3];
+    LocalPlan<double> lp64{};
+    LocalPlan<float> lp32{};
+};
+
+class Context {
+  public:
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    size_t budget = 0;
+    size_t held = 0;
+    std::string err;
+
+    int n1 = 0, n2 = 0, n3 = 0;
+    bool pot_valid = false;
+    std::vector<double> v_host;     // V(r) as given, reference layout
+    DevBuf v64, v32;                // V/N, [w3][w1][w2]
+
+    KPoint kp;
+
+    // workspaces
+    DevBuf ws_sticks, ws_gemm, ws_bm, ws_bp, ws_conv_in, ws_conv_out, ws_host_io;
+
+    explicit Context(int dev, size_t hbm_budget);
+    ~Context();
+
+    void set_potential(const double* v, int a, int b, int c);
+    void prepare_kpoint(int npw, const int32_t* g2g, const double* ke, const double2* beta, int nproj,
+                        int natoms, const int32_t* offs, const double* dblk);
+    void require_ready() const;
+
+    template <typename R> const LocalPlan<R>& local_plan() const;
+    template <typename R> NonlocalData<R> nonlocal() const;
+    template <typename R> int sticks_chunk(int nvec) const;
+
+    // H|psi> on device vectors in precision R (the solver's building block)
+    template <typename R>
+    void apply_h(const cplx_t<R>* psi, long ldpsi, cplx_t<R>* hpsi, long ldh, int nvec);
+
+    GemmWorkspace gemm_ws(size_t need);
+
+  private:
+    void build_plan();
+};
+
+// convert an exception into a status code and message
+int fail(q3b_context* c, const std::exception& e);
+
+}  // namespace q3b
+
+struct q3b_context {
+    q3b::Context impl;
+    q3b_context(int dev, size_t budget) : impl(dev, budget) {}
+};

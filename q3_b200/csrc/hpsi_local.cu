@@ -1,0 +1,188 @@
+// Kinetic + local-potential part of H|psi>; see hpsi_local.cuh.
+//
+// Follows SerialPlanewaveHamiltonianApplicator::apply_hamiltonian_batch
+// (hamiltonian_applicator/serial.hpp:450-477): hpsi = KE*psi, scatter psi by
+// the G->grid map, unnormalised backward 3D FFT, multiply by V/N, unnormalised
+// forward 3D FFT, hpsi += grid[map].  The 3D transforms are factored into
+// stick (w3) and plane (w1, w2) transforms that never touch empty sticks.
+#include <mutex>
+
+#include "fft_core.cuh"
+#include "hpsi_local.cuh"
+
+namespace q3b {
+namespace {
+
+constexpr int kStickThreads = 256;
+constexpr int kPlaneThreads = 256;
+
+template <typename R> struct VEpilogue {
+    const R* vp;  // V/N of this plane, [w1][w2]
+    int n2;
+    template <typename T> __device__ __forceinline__ T operator()(int l, int j, T v) const {
+        const R s = vp[j * n2 + l];
+        return s * v;
+    }
+};
+
+// pass A: scatter + backward transform along w3, store X[band][w3][stick]
+template <typename R>
+__global__ void __launch_bounds__(kStickThreads)
+sticks_backward(LocalPlan<R> p, const cplx_t<R>* __restrict__ psi, long ldpsi, cplx_t<R>* X) {
+    using T = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* tw = reinterpret_cast<T*>(smem);
+    T* lines = tw + p.n3;
+    const int band = blockIdx.y;
+    const int s0 = blockIdx.x * p.sg;
+    const int ns = min(p.sg, p.nsticks - s0);
+    for (int i = threadIdx.x; i < p.n3; i += blockDim.x) tw[i] = p.tw3[i];
+    for (int i = threadIdx.x; i < ns * p.p3; i += blockDim.x) lines[i] = czero<T>();
+    __syncthreads();
+    const T* ps = psi + (long)band * ldpsi;
+    const int e0 = p.stick_start[s0], e1 = p.stick_start[s0 + ns];
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        lines[(p.entry_stick[e] - s0) * p.p3 + p.entry_w3[e]] = ps[p.entry_g[e]];
+    }
+    __syncthreads();
+    fft::LineGeom g{p.n3, p.na3, p.nb3, ns, p.p3, 1, nullptr};
+    fft::lines<+1, 1>(lines, g, tw, fft::NoEpilogue{});
+    T* xb = X + (long)band * p.n3 * p.nsticks;
+    for (int idx = threadIdx.x; idx < ns * p.n3; idx += blockDim.x) {
+        const int s = idx % ns, i3 = idx / ns;
+        xb[(long)i3 * p.nsticks + s0 + s] = lines[s * p.p3 + i3];
+    }
+}
+
+// pass B: one (band, w3) plane per block
+template <typename R>
+__global__ void __launch_bounds__(kPlaneThreads) planes(LocalPlan<R> p, cplx_t<R>* X) {
+    using T = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* tw1 = reinterpret_cast<T*>(smem);
+    T* tw2 = tw1 + p.n1;
+    T* plane = tw2 + p.n2;
+    int* rowb = reinterpret_cast<int*>(plane + (long)p.n1 * p.p2);
+    const int i3 = blockIdx.x, band = blockIdx.y;
+    for (int i = threadIdx.x; i < p.n1; i += blockDim.x) tw1[i] = p.tw1[i];
+    for (int i = threadIdx.x; i < p.n2; i += blockDim.x) tw2[i] = p.tw2[i];
+    for (int i = threadIdx.x; i < p.nrows; i += blockDim.x) rowb[i] = p.row_base[i];
+    for (int i = threadIdx.x; i < p.n1 * p.p2; i += blockDim.x) plane[i] = czero<T>();
+    __syncthreads();
+    T* xp = X + ((long)band * p.n3 + i3) * p.nsticks;
+    for (int s = threadIdx.x; s < p.nsticks; s += blockDim.x) plane[p.stick_pos[s]] = xp[s];
+    __syncthreads();
+    fft::LineGeom gr{p.n2, p.na2, p.nb2, p.nrows, 0, 1, rowb};
+    fft::LineGeom gc{p.n1, p.na1, p.nb1, p.n2, 1, p.p2, nullptr};
+    fft::lines<+1, 1>(plane, gr, tw2, fft::NoEpilogue{});
+    fft::lines<+1, 1>(plane, gc, tw1, VEpilogue<R>{p.vplane + (long)i3 * p.n1 * p.n2, p.n2});
+    fft::lines<-1, 1>(plane, gc, tw1, fft::NoEpilogue{});
+    fft::lines<-1, 1>(plane, gr, tw2, fft::NoEpilogue{});
+    for (int s = threadIdx.x; s < p.nsticks; s += blockDim.x) xp[s] = plane[p.stick_pos[s]];
+}
+
+// pass C: forward transform along w3, gather the sphere, add the kinetic term
+template <typename R>
+__global__ void __launch_bounds__(kStickThreads)
+sticks_forward(LocalPlan<R> p, const cplx_t<R>* __restrict__ X, const cplx_t<R>* __restrict__ psi,
+               long ldpsi, cplx_t<R>* hpsi, long ldh) {
+    using T = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* tw = reinterpret_cast<T*>(smem);
+    T* lines = tw + p.n3;
+    const int band = blockIdx.y;
+    const int s0 = blockIdx.x * p.sg;
+    const int ns = min(p.sg, p.nsticks - s0);
+    for (int i = threadIdx.x; i < p.n3; i += blockDim.x) tw[i] = p.tw3[i];
+    const T* xb = X + (long)band * p.n3 * p.nsticks;
+    for (int idx = threadIdx.x; idx < ns * p.n3; idx += blockDim.x) {
+        const int s = idx % ns, i3 = idx / ns;
+        lines[s * p.p3 + i3] = xb[(long)i3 * p.nsticks + s0 + s];
+    }
+    __syncthreads();
+    fft::LineGeom g{p.n3, p.na3, p.nb3, ns, p.p3, 1, nullptr};
+    fft::lines<-1, 1>(lines, g, tw, fft::NoEpilogue{});
+    const T* ps = psi + (long)band * ldpsi;
+    T* hs = hpsi + (long)band * ldh;
+    const int e0 = p.stick_start[s0], e1 = p.stick_start[s0 + ns];
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const int gi = p.entry_g[e];
+        const T v = lines[(p.entry_stick[e] - s0) * p.p3 + p.entry_w3[e]];
+        hs[gi] = p.ke[gi] * ps[gi] + v;
+    }
+}
+
+// G outside the grid get the kinetic term only (serial.hpp:451-462 skip them)
+template <typename R>
+__global__ void kinetic_unmapped(LocalPlan<R> p, const cplx_t<R>* psi, long ldpsi, cplx_t<R>* hpsi,
+                                 long ldh, int nvec) {
+    const long total = (long)p.nunmapped * nvec;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long)gridDim.x * blockDim.x) {
+        const int i = static_cast<int>(idx % p.nunmapped);
+        const long b = idx / p.nunmapped;
+        const int gi = p.unmapped_g[i];
+        hpsi[b * ldh + gi] = p.ke[gi] * psi[b * ldpsi + gi];
+    }
+}
+
+template <typename R> size_t stick_smem_bytes(const LocalPlan<R>& p) {
+    return (size_t)(p.n3 + p.sg * p.p3) * sizeof(cplx_t<R>);
+}
+
+template <typename R> void set_smem_limits() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const int lim = 227 * 1024;
+        cudaFuncSetAttribute(planes<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(sticks_backward<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(sticks_forward<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    });
+}
+
+}  // namespace
+
+template <typename R> size_t plane_smem_bytes(const LocalPlan<R>& p) {
+    return (size_t)(p.n1 + p.n2 + (size_t)p.n1 * p.p2) * sizeof(cplx_t<R>) +
+           (size_t)p.nrows * sizeof(int);
+}
+
+template <typename R>
+void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, long ldpsi,
+                 cplx_t<R>* hpsi, long ldh, int nvec, cplx_t<R>* X, int chunk) {
+    if (nvec <= 0) return;
+    set_smem_limits<R>();
+    if (chunk < 1) chunk = 1;
+    const size_t smem_s = stick_smem_bytes(p);
+    const size_t smem_p = plane_smem_bytes(p);
+    const int nsg = ceil_div(p.nsticks, p.sg);
+    for (int b0 = 0; b0 < nvec; b0 += chunk) {
+        const int nb = nvec - b0 < chunk ? nvec - b0 : chunk;
+        const cplx_t<R>* ps = psi + (long)b0 * ldpsi;
+        cplx_t<R>* hs = hpsi + (long)b0 * ldh;
+        if (p.nsticks > 0) {
+            sticks_backward<R><<<dim3(nsg, nb), kStickThreads, smem_s, st>>>(p, ps, ldpsi, X);
+            Q3B_LAUNCH_CHECK();
+            planes<R><<<dim3(p.n3, nb), kPlaneThreads, smem_p, st>>>(p, X);
+            Q3B_LAUNCH_CHECK();
+            sticks_forward<R><<<dim3(nsg, nb), kStickThreads, smem_s, st>>>(p, X, ps, ldpsi, hs, ldh);
+            Q3B_LAUNCH_CHECK();
+        }
+    }
+    if (p.nunmapped > 0) {
+        const long total = (long)p.nunmapped * nvec;
+        int blocks = ceil_div(total, 256);
+        if (blocks > 1024) blocks = 1024;
+        kinetic_unmapped<R><<<blocks, 256, 0, st>>>(p, psi, ldpsi, hpsi, ldh, nvec);
+        Q3B_LAUNCH_CHECK();
+    }
+}
+
+template void apply_local<double>(cudaStream_t, const LocalPlan<double>&, const double2*, long,
+                                  double2*, long, int, double2*, int);
+template void apply_local<float>(cudaStream_t, const LocalPlan<float>&, const float2*, long,
+                                 float2*, long, int, float2*, int);
+template size_t plane_smem_bytes<double>(const LocalPlan<double>&);
+template size_t plane_smem_bytes<float>(const LocalPlan<float>&);
+
+}  // namespace q3b

@@ -1,0 +1,58 @@
+// Kinetic + local-potential part of H|psi> on the sticks/planes layout.
+//
+// A k-point's G-sphere occupies S "sticks" (grid columns (w1, w2) along the
+// contiguous axis w3).  One application for a chunk of bands is three kernels:
+//   A  sticks, backward: scatter psi into each stick, 1D transform along w3,
+//      store X[band][w3][stick];
+//   B  planes: per (band, w3) plane in shared memory, scatter the S stick
+//      values, 2D backward transform (rows w1 that hold sticks, then all
+//      columns), multiply by V(r)/N, 2D forward transform, gather back;
+//   C  sticks, forward: 1D forward transform along w3, gather the sphere and
+//      write hpsi = |k+G|^2 psi + (local term).
+// Nothing outside the sticks is stored or moved through HBM.
+#pragma once
+
+#include "common.cuh"
+
+namespace q3b {
+
+template <typename R> struct LocalPlan {
+    using T = cplx_t<R>;
+    int n1, n2, n3;
+    int npw;
+    int nsticks;
+    int nrows;          // distinct w1 among the sticks
+    int p2;             // pitch of a plane row in shared memory (odd)
+    int p3;             // pitch of a stick line in shared memory (odd)
+    int na1, nb1, na2, nb2, na3, nb3;
+    int sg;             // sticks per block in passes A and C
+    int nunmapped;      // G outside the grid: kinetic term only
+    const int* stick_start;  // nsticks+1, ranges into the entry arrays
+    const int* entry_g;      // G index (caller's order) of each sphere entry
+    const int* entry_w3;
+    const int* entry_stick;
+    const int* stick_pos;    // w1*p2 + w2
+    const int* row_base;     // w1*p2 of each used row
+    const int* unmapped_g;
+    const T* tw1;            // w_n^m = exp(-2 pi i m/n), one table per axis
+    const T* tw2;
+    const T* tw3;
+    const R* ke;             // |k+G|^2 (Ry), caller's order
+    const R* vplane;         // V(r)/N laid out [w3][w1][w2]
+};
+
+// bytes of the stick buffer per band
+template <typename R> inline size_t sticks_bytes_per_band(const LocalPlan<R>& p) {
+    return (size_t)p.n3 * p.nsticks * sizeof(cplx_t<R>);
+}
+
+// hpsi[:, b] = KE*psi[:, b] + local term, for nvec bands (column stride ld).
+// X must hold chunk*sticks_bytes_per_band bytes.
+template <typename R>
+void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, long ldpsi,
+                 cplx_t<R>* hpsi, long ldh, int nvec, cplx_t<R>* X, int chunk);
+
+// shared-memory footprint of the plane kernel (for capacity checks)
+template <typename R> size_t plane_smem_bytes(const LocalPlan<R>& p);
+
+}  // namespace q3b

@@ -1,0 +1,28 @@
+// Kleinman-Bylander nonlocal term of H|psi>; see nonlocal.cu.
+#pragma once
+
+#include "cgemm.cuh"
+#include "common.cuh"
+
+namespace q3b {
+
+template <typename R> struct NonlocalData {
+    int nproj = 0;
+    const cplx_t<R>* beta = nullptr;  // npw x nproj, ld npw
+    const int* pstart = nullptr;      // first projector of p's atom block
+    const int* psize = nullptr;       // size of p's atom block
+    const int* poff = nullptr;        // offset of p's block in dpk
+    const R* dpk = nullptr;           // packed column-major D blocks (Ry)
+};
+
+// hpsi += beta D beta^H psi.  Bm, Bp: nproj x nvec scratch each.
+template <typename R>
+void apply_nonlocal(cudaStream_t st, const NonlocalData<R>& nl, int npw, int nvec,
+                    const cplx_t<R>* psi, long ldpsi, cplx_t<R>* hpsi, long ldh, cplx_t<R>* Bm,
+                    cplx_t<R>* Bp, const GemmWorkspace& ws);
+
+// out = (RO) in, n complex values
+template <typename RI, typename RO>
+void convert(cudaStream_t st, long n, const cplx_t<RI>* in, cplx_t<RO>* out);
+
+}  // namespace q3b

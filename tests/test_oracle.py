@@ -1,0 +1,167 @@
+"""The CPU oracle against the reference's own known-answer tests for this path.
+
+The reference's tests hold no golden H|psi> or Davidson vectors for these
+cells; they pin the FFT convention (test_fft_grid.cpp:13-83) and the subspace
+eigensolver (test_subspace_diagonalizer.cpp:11-166).  Those are replayed here
+on the oracle, plus structural checks (H Hermitian, the local term equal to
+its plane-wave matrix elements V(G'-G), Davidson equal to dense
+diagonalisation).
+"""
+import math
+
+import numpy as np
+import pytest
+import scipy.fft as sfft
+
+from oracle import davidson, hpsi
+from q3_b200 import synthetic
+
+
+def fftw_backward(x):
+    return sfft.ifftn(x, norm="forward")
+
+
+def fftw_forward(x):
+    return sfft.fftn(x, norm="backward")
+
+
+def test_fft_round_trip_kat():
+    # test_fft_grid.cpp:13-42 -- cos(2 pi x / L) on 16^3, forward then normalised inverse
+    n = 16
+    i1 = np.arange(n)[None, None, :]
+    data = np.broadcast_to(np.cos(2 * np.pi * i1 / n), (n, n, n)).astype(np.complex128)
+    back = fftw_backward(fftw_forward(data)) / data.size
+    assert np.max(np.abs(back - data)) < 1e-10
+
+
+def test_fft_parseval_kat():
+    # test_fft_grid.cpp:54-83 -- sum |f|^2 = (1/N) sum |F|^2 on 12^3
+    n = 12
+    i = np.arange(n ** 3)
+    data = (np.sin(0.3 * i + 0.7) + 1j * np.cos(0.5 * i - 0.2)).reshape(n, n, n)
+    sr = np.sum(np.abs(data) ** 2)
+    sg = np.sum(np.abs(fftw_forward(data)) ** 2)
+    assert abs(sr - sg / data.size) < 1e-6 * sr
+
+
+def test_fft_sign_convention():
+    # FFTW_BACKWARD is e^{+i}: a single coefficient at G=1 gives exp(+2 pi i x / n)
+    n = 8
+    g = np.zeros((n, n, n), complex)
+    g[0, 0, 1] = 1.0
+    r = fftw_backward(g)
+    x = np.arange(n)
+    assert np.allclose(r[0, 0, :], np.exp(2j * np.pi * x / n))
+
+
+def _solve(h, s):
+    w, v, info = davidson.diagonalize_subspace(np.asarray(h, complex), np.asarray(s, complex), len(h))
+    return w, v, info
+
+
+def test_subspace_kat_identity():
+    # test_subspace_diagonalizer.cpp:11-29
+    w, v, info = _solve([[2, 0], [0, 3]], np.eye(2))
+    assert info == 0 and abs(w[0] - 2) < 1e-10 and abs(w[1] - 3) < 1e-10
+
+
+def test_subspace_kat_generalized():
+    # test_subspace_diagonalizer.cpp:31-56 -- H=diag(2,4), S=diag(1,2): both 2
+    w, v, info = _solve([[2, 0], [0, 4]], [[1, 0], [0, 2]])
+    assert info == 0 and abs(w[0] - 2) < 1e-10 and abs(w[1] - 2) < 1e-10
+
+
+def test_subspace_kat_real_symmetric():
+    # test_subspace_diagonalizer.cpp:58-86 -- [[2,1],[1,2]]: 1 and 3
+    w, v, info = _solve([[2, 1], [1, 2]], np.eye(2))
+    assert info == 0 and abs(w[0] - 1) < 1e-10 and abs(w[1] - 3) < 1e-10
+
+
+def generalized_problem_48(n=48):
+    """test_subspace_diagonalizer.cpp:88-113: the 48x48 Hermitian / HPD pair."""
+    h = np.zeros((n, n), complex)
+    s = np.zeros((n, n), complex)
+    for col in range(n):
+        for row in range(col + 1):
+            re = math.sin(0.37 * (row + 1) + 0.11 * (col + 1) * (col + 1))
+            im = 0.0 if row == col else math.cos(0.23 * (row + 2) * (col + 1))
+            h[row, col] = re + 1j * im
+            h[col, row] = re - 1j * im
+            c = (2.0 + 0.01 * row) if row == col else (0.02 * re + 0.02j * im)
+            s[row, col] = c
+            s[col, row] = np.conj(c)
+        h[col, col] += 0.5 * col
+    return h, s
+
+
+def test_subspace_kat_48():
+    # test_subspace_diagonalizer.cpp:115-160: every eigenvector solves H c = e S c to 1e-10
+    h, s = generalized_problem_48()
+    w, v, info = _solve(h, s)
+    assert info == 0
+    assert np.all(np.diff(w) >= 0)
+    res = h @ v - (s @ v) * w[None, :]
+    assert np.max(np.abs(res)) < 1e-10
+    # S-orthonormal
+    assert np.max(np.abs(v.conj().T @ s @ v - np.eye(48))) < 1e-10
+
+
+def test_config0_sizes():
+    # npw of the full sphere at 30 Ry in the FCC cell, and its sticks
+    sy = synthetic.config(0)
+    kp = sy.kpoints[0]
+    assert kp.npw == 725 and kp.nproj == 16
+    cols = {(int(m[0]) % 24, int(m[1]) % 24) for m in kp.miller}
+    assert len(cols) == 109
+    assert np.all(kp.g_to_grid >= 0)
+
+
+def test_local_term_equals_plane_wave_matrix_elements():
+    # <G'|V|G> = V(G'-G) with V(G) = (1/N) sum_r V(r) e^{-iGr}: an independent
+    # statement of serial.hpp:457-477
+    sy = synthetic.small_system(grid=(10, 10, 10), a=6.0, ecut=6.0, nbands=4)
+    kp = sy.kpoints[0]
+    n = sy.cell.grid
+    vg = sfft.fftn(sy.v_r.reshape(n)) / sy.cell.npoints
+    m = kp.miller
+    npw = kp.npw
+    dm = (m[:, None, :] - m[None, :, :]) % np.array(n)[None, None, :]
+    vmat = vg[dm[..., 0], dm[..., 1], dm[..., 2]]
+    hmat = np.diag(kp.ke).astype(complex) + vmat
+    rng = np.random.default_rng(3)
+    psi = rng.standard_normal((npw, 3)) + 1j * rng.standard_normal((npw, 3))
+    got = hpsi.apply_local(psi, kp.ke, kp.g_to_grid, sy.v_r, n)
+    assert np.max(np.abs(got - hmat @ psi)) < 1e-11 * np.max(np.abs(got))
+
+
+def test_oracle_h_hermitian_and_nonlocal():
+    sy = synthetic.small_system(grid=(12, 12, 12), a=7.0, ecut=8.0, nbands=4)
+    kp = sy.kpoints[0]
+    hd = hpsi.dense_hamiltonian(kp, sy.v_r, sy.cell.grid)
+    assert np.max(np.abs(hd - hd.conj().T)) < 1e-12 * np.max(np.abs(hd))
+    # nonlocal = beta D beta^H
+    nl = kp.beta @ kp.d_dense() @ kp.beta.conj().T
+    eye = np.eye(kp.npw, dtype=complex)
+    got = hpsi.apply_nonlocal(eye, kp.beta, kp.d_blocks, kp.atom_proj_offsets)
+    assert np.max(np.abs(got - nl)) < 1e-12
+
+
+def test_oracle_davidson_matches_dense():
+    sy = synthetic.small_system(grid=(12, 12, 12), a=7.0, ecut=8.0, nbands=6)
+    kp = sy.kpoints[0]
+    hd = hpsi.dense_hamiltonian(kp, sy.v_r, sy.cell.grid)
+    exact = np.linalg.eigvalsh(hd)[:6]
+    res = davidson.solve(lambda x: hd @ x, kp.ke, sy.psi0[0], 6, tolerance=1e-11,
+                         max_iterations=80)
+    assert res.unconverged == 0
+    assert np.max(np.abs(res.eigenvalues - exact)) < 1e-9
+
+
+def test_oracle_davidson_seeds_from_kinetic_energy():
+    # zero starting bands are replaced by the lowest-KE plane waves (davidson.hpp:1047-1101)
+    sy = synthetic.small_system(grid=(12, 12, 12), a=7.0, ecut=8.0, nbands=5)
+    kp = sy.kpoints[0]
+    hd = hpsi.dense_hamiltonian(kp, sy.v_r, sy.cell.grid)
+    exact = np.linalg.eigvalsh(hd)[:5]
+    res = davidson.solve(lambda x: hd @ x, kp.ke, None, 5, tolerance=1e-11, max_iterations=80)
+    assert np.max(np.abs(res.eigenvalues - exact)) < 1e-9
