@@ -1,0 +1,436 @@
+#!/usr/bin/env python
+"""Benchmark: band H|psi> applications/s and Davidson solves/s on one B200 per rank.
+
+Workload (N = 1): the single-cell H|psi> configuration -- a simple-cubic
+64-atom cell, a = 20.5 bohr, Gamma, ecutwfc 15 Ha (23,847 plane waves), FFT
+grid 80^3, 256 bands, 512 Kleinman-Bylander projectors -- with seeded
+synthetic inputs (q3_b200.synthetic).  One step = one H|psi> application to
+the 256-band block.  `value` is the mixed-precision (FP32 H|psi>) band
+throughput with inputs resident in HBM, device-timed with CUDA events, L2
+flushed between steps; the FP64 figure, the per-kernel breakdown, the
+Davidson solves (FP64 and mixed, eigenvalue error of the mixed solve against
+the FP64 one) and the end-to-end figure through the host C ABI are reported
+beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl q3b|reference]
+
+With N > 1 (torchrun) every rank solves its own copy of the workload
+(independent cells: weak scaling, no collective on the data path); rank 0
+prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "band H|psi>/s (mixed FP32 H|psi>, 256-band block)"
+UNIT = "band-applications/s"
+WORKLOAD = ("SC 64-atom cell a=20.5 bohr, Gamma, ecut 15 Ha (npw 23847), FFT 80^3, "
+            "256 bands, 512 KB projectors")
+L2_FLUSH_BYTES = 512 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["q3b", "reference"], default="q3b")
+    ap.add_argument("--no-davidson", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--davidson-tol", type=float, default=1e-9, help="Ry")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", self.gpu_id],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def gpu_id_for(dev_index: int) -> str:
+    import torch
+    try:
+        u = torch.cuda.get_device_properties(dev_index).uuid
+        return "GPU-" + str(u)
+    except Exception:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        if vis:
+            return vis.split(",")[dev_index]
+        return str(dev_index)
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def traffic_table():
+    p = ROOT / "profiles" / "traffic.json"
+    return json.loads(p.read_text()) if p.exists() else {}
+
+
+# ----------------------------------------------------------- algorithmic bytes
+def kernel_bytes(kp, grid, nsticks, nvec, c, r):
+    """Algorithmic bytes per launch class for nvec bands (c: complex, r: real size).
+
+    Sticks model: a stick carries N3 values; pass A reads psi and writes the
+    sticks, pass B reads and writes them, pass C reads them, reads psi and
+    writes H psi.  V (N reals) is read once per band by the planes."""
+    n1, n2, n3 = grid
+    npw, P = kp.npw, kp.nproj
+    st = nsticks * n3 * c
+    return {
+        "sticks_backward": nvec * (npw * c + st),
+        "planes": nvec * (2 * st + n1 * n2 * n3 * r),
+        "sticks_forward": nvec * (st + 2 * npw * c) + npw * r,
+        "projector_overlap": (npw * P + npw * nvec) * c + P * nvec * c,
+        "projector_accumulate": (npw * P + P * nvec + 2 * npw * nvec) * c,
+        "d_apply": 2 * P * nvec * c,
+    }
+
+
+def kernel_flops(kp, nvec):
+    return {"projector_overlap": 8.0 * kp.npw * kp.nproj * nvec,
+            "projector_accumulate": 8.0 * kp.npw * kp.nproj * nvec}
+
+
+# ------------------------------------------------------------------ oracle CPU
+def cpu_sample(sy, bands: int, min_seconds: float, max_seconds: float):
+    """Oracle H|psi> (the reference's CPU algorithm restated) on all host cores."""
+    from oracle import hpsi as ohpsi
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(threads))
+    kp = sy.kpoints[0]
+    psi = np.asfortranarray(sy.psi0[0][:, :bands])
+    done, t0 = 0, time.perf_counter()
+    while True:
+        ohpsi.apply_h(psi, kp, sy.v_r, sy.cell.grid, threads=threads)
+        done += bands
+        el = time.perf_counter() - t0
+        if el >= min_seconds or el >= max_seconds:
+            break
+    return done / el, threads, f"{done} band applications ({bands}-band batches) of the same cell, {el:.1f} s"
+
+
+def run_reference(args):
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    from q3_b200 import synthetic
+    sy = synthetic.config(1)
+    vals = []
+    cores = os.cpu_count() or 1
+    sample = ""
+    for _ in range(max(1, args.warmup)):
+        cpu_sample(sy, 4, 0.0, 0.0)
+    for _ in range(args.steps):
+        v, cores, sample = cpu_sample(sy, 16, 0.0, 0.0)
+        vals.append(v)
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 16.0 / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "step": "16-band sample per step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------- q3b arm
+def run_q3b(args):
+    import torch
+    from q3_b200 import synthetic
+    from q3_b200._lib import FP64, MIXED, ApplyTiming, check
+    from q3_b200.applicator import PlanewaveHamiltonianApplicator
+    from q3_b200.davidson import PlanewaveDavidsonDiagonalizer
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    dev = torch.device("cuda", local)
+
+    sy = synthetic.config(1)
+    kp = sy.kpoints[0]
+    nb = sy.nbands
+    ap = PlanewaveHamiltonianApplicator(device=local)
+    ap.update_potential(sy.v_r, sy.cell.grid)
+    ap.prepare_system_kpoint(sy)
+    lib, h = ap.lib, ap.h
+    stream = torch.cuda.ExternalStream(ap.ctx.stream, device=dev)
+
+    psi64 = torch.from_numpy(np.ascontiguousarray(sy.psi0[0].T)).to(dev)
+    hpsi64 = torch.empty_like(psi64)
+    psi32 = psi64.to(torch.complex64)
+    hpsi32 = torch.empty_like(psi32)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def step32():
+        check(h, lib.q3b_apply_h_f32(h, psi32.data_ptr(), hpsi32.data_ptr(), nb))
+
+    def step64():
+        check(h, lib.q3b_apply_h(h, psi64.data_ptr(), hpsi64.data_ptr(), nb, FP64))
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def timed(fn, k):
+        """k steps, L2 flushed before each, device time of the steps only (ms, max over ranks)."""
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k)]
+        barrier()
+        torch.cuda.synchronize()
+        for i in range(k):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(i))
+            ev[i][0].record(stream)
+            fn()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+        if pg is not None:
+            t = torch.tensor([ms], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    for _ in range(max(3, args.warmup)):
+        step32()
+        step64()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(gpu_id_for(local))
+    clocks.start()
+    time.sleep(0.3)
+    l0 = lib.q3b_kernel_launches()
+    ms32 = timed(step32, args.steps)
+    launches = int(lib.q3b_kernel_launches() - l0) // max(1, args.steps) * args.steps
+    ms64 = timed(step64, args.steps)
+    clocks.stop()
+    value = world * nb / (ms32 * 1e-3)
+    value64 = world * nb / (ms64 * 1e-3)
+
+    # per-kernel breakdown (CUDA events around each launch)
+    def breakdown(fp32):
+        t = ApplyTiming()
+        with torch.cuda.stream(stream):
+            flush.fill_(0.5)
+        x, y = (psi32, hpsi32) if fp32 else (psi64, hpsi64)
+        check(h, lib.q3b_apply_h_timed(h, x.data_ptr(), y.data_ptr(), nb, 1 if fp32 else 0, t))
+        return t.as_dict()
+
+    k32 = breakdown(True)
+    k64 = breakdown(False)
+
+    # correctness guard: FP32 and FP64 H|psi> agree to single precision
+    rel = float((hpsi32.to(torch.complex128) - hpsi64).abs().max() / hpsi64.abs().max())
+
+    # end to end through the host C ABI (pinned host buffers, copies timed)
+    hin = torch.from_numpy(np.ascontiguousarray(sy.psi0[0].T)).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    for _ in range(2):
+        check(h, lib.q3b_apply_h_host(h, hin.data_ptr(), hout.data_ptr(), nb, MIXED))
+    e2e_ms = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        check(h, lib.q3b_apply_h_host(h, hin.data_ptr(), hout.data_ptr(), nb, MIXED))
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    e2e = float(np.mean(e2e_ms))
+    if pg is not None:
+        t = torch.tensor([e2e], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e = float(t.item())
+    io_bytes = nb * kp.npw * 16
+
+    # Davidson solves, FP64 and mixed, on the same cell
+    dav = None
+    if not args.no_davidson:
+        def solve(prec):
+            d = PlanewaveDavidsonDiagonalizer(ap, prec)
+            d.set_tolerance(args.davidson_tol)
+            d.set_maximum_iterations(100)
+            if prec == MIXED:
+                d.set_precision(MIXED, 1e-5, 12)
+            x = psi64.clone()
+            torch.cuda.synchronize()
+            r = d.solve(x, nb)
+            return r
+        r64 = solve(FP64)
+        rmx = solve(MIXED)
+        err_ry = float(np.max(np.abs(rmx.eigenvalues - r64.eigenvalues)))
+        dav = {
+            "tolerance_ry": args.davidson_tol,
+            "fp64": {"solves_per_s": world / r64.seconds, "seconds": r64.seconds,
+                     "iterations": r64.iterations, "ms_per_iteration": 1e3 * r64.seconds / max(1, r64.iterations),
+                     "h_applications": r64.h_applications, "max_residual_norm": r64.max_residual_norm,
+                     "unconverged": r64.unconverged},
+            "mixed": {"solves_per_s": world / rmx.seconds, "seconds": rmx.seconds,
+                      "iterations": rmx.iterations, "fp64_iterations": rmx.fp64_iterations,
+                      "ms_per_iteration": 1e3 * rmx.seconds / max(1, rmx.iterations),
+                      "h_applications": rmx.h_applications, "max_residual_norm": rmx.max_residual_norm,
+                      "unconverged": rmx.unconverged},
+            "mixed_vs_fp64_max_eig_err_ha": err_ry / 2.0,
+            "mixed_speedup": r64.seconds / rmx.seconds,
+        }
+
+    if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
+    # roofline of the dominant kernel of the mixed step
+    hbm, bf16, peak_kind = measured_peaks()
+    nsticks = None
+    kb32 = None
+    name, (ms_dom, n_dom) = max(k32.items(), key=lambda kv: kv[1][0])
+    from q3_b200.plan_info import stick_count
+    nsticks = stick_count(kp, sy.cell.grid)
+    kb32 = kernel_bytes(kp, sy.cell.grid, nsticks, nb, 8, 4)
+    traffic = traffic_table().get(f"config1/{name}/fp32")
+    if name in ("projector_overlap", "projector_accumulate"):
+        fl = kernel_flops(kp, nb)[name]
+        achieved = fl / (ms_dom * 1e-3) / 1e12
+        roof = {"kernel": name, "bound": "tensor", "achieved": achieved, "peak": bf16 / 2.0,
+                "unit": "TFLOP/s", "frac": achieved / (bf16 / 2.0),
+                "peak_note": f"TF32 = half of {peak_kind} bf16", "traffic": traffic,
+                "launches": n_dom, "ms": ms_dom}
+    else:
+        per_launch = kb32[name] / max(1, n_dom)
+        achieved = kb32[name] / (ms_dom * 1e-3) / 1e9
+        roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_note": f"{peak_kind} copy bandwidth",
+                "algorithmic_bytes_per_launch": per_launch, "traffic": traffic,
+                "launches": n_dom, "ms": ms_dom}
+
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        v, cores, sample = cpu_sample(sy, 16, 10.0, 30.0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+
+    cs = clocks.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, q3_b200.synthetic)",
+        "config": {"workload": WORKLOAD, "bands": nb, "npw": kp.npw, "projectors": kp.nproj,
+                   "grid": list(sy.cell.grid), "sticks": nsticks,
+                   "l2": "flushed (512 MiB write) before every timed step",
+                   "parallelism": f"replicas x{world}"},
+        "fp64": {"value": value64, "ms_per_step": ms64, "dtype": "f64"},
+        "fp32_vs_fp64_rel_diff": rel,
+        "kernels_fp32_ms": {k: v[0] for k, v in k32.items()},
+        "kernels_fp64_ms": {k: v[0] for k, v in k64.items()},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * nb / (e2e * 1e-3), "unit": UNIT, "ms_per_step": e2e,
+                "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes,
+                "path": "q3b_apply_h_host, pinned FP64 host buffers, MIXED"},
+        "gpu_launches": launches,
+        "clocks": cs,
+        "davidson": dav,
+    }
+    print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_q3b(args)
+
+
+if __name__ == "__main__":
+    main()

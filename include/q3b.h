@@ -104,6 +104,77 @@ int q3b_apply_h_f32(q3b_context* ctx, const q3b_cplx64* psi_dev, q3b_cplx64* hps
 int q3b_apply_h_host(q3b_context* ctx, const q3b_cplx128* psi_host, q3b_cplx128* hpsi_host,
                      int nvec, int precision);
 
+/* ---- diagnostics ---------------------------------------------------------- */
+
+/* Per-kernel device time of one application, CUDA events around each launch
+ * (the reference's hamiltonian_fft / nonlocal / projector_overlap timers,
+ * counters.hpp:36-52, split by kernel). */
+typedef struct {
+    double sticks_backward_ms;       /* scatter + backward transform along w3     */
+    double planes_ms;                /* 2D transforms + V(r) product              */
+    double sticks_forward_ms;        /* forward transform along w3 + gather + KE  */
+    double projector_overlap_ms;     /* <beta|psi>                                */
+    double d_apply_ms;               /* D blocks                                  */
+    double projector_accumulate_ms;  /* hpsi += beta (D <beta|psi>)              */
+    int launches[6];                 /* launches of each of the six classes       */
+} q3b_apply_timing;
+
+/* q3b_apply_h (fp32 == 0, cplx128 vectors) or q3b_apply_h_f32 (fp32 != 0,
+ * cplx64 vectors) with the timing above; synchronises the stream. */
+int q3b_apply_h_timed(q3b_context* ctx, const void* psi_dev, void* hpsi_dev, int nvec, int fp32,
+                      q3b_apply_timing* timing);
+
+/* Kernel launches the library has issued in this process (all contexts). */
+unsigned long long q3b_kernel_launches(void);
+
+/* ---- PlanewaveDavidsonDiagonalizer::solve -------------------------------- */
+
+typedef struct {
+    double tolerance;            /* eigenvalue-change tolerance, Ry (davidson.hpp:608-629)  */
+    int max_iterations;          /* set_maximum_iterations (davidson.hpp:270-272), default 20 */
+    int basis_expansion_factor;  /* set_basis_expansion_factor (davidson.hpp:260-264), >= 2 */
+    int occupied_bands;          /* bands held to `tolerance`; the rest to max(5 tol, 1e-5)  */
+    int precision;               /* Q3B_FP64 or Q3B_MIXED                                   */
+    int refine_sweeps;           /* MIXED: max FP64 refinement iterations at the end         */
+    double mixed_tolerance;      /* MIXED: eigenvalue-change tolerance of the FP32 phase, Ry */
+} q3b_davidson_opts;
+
+typedef struct {
+    int iterations;              /* Davidson iterations run (both phases)                   */
+    int fp64_iterations;         /* of which in FP64                                        */
+    int h_applications;          /* band applications of H                                  */
+    int unconverged;             /* bands short of the tolerance at exit                    */
+    int collapses;
+    double max_residual_norm;    /* max_i ||H psi_i - eps_i psi_i|| of the returned bands   */
+    double seconds;              /* wall time of the solve                                   */
+} q3b_davidson_stats;
+
+void q3b_davidson_default_opts(q3b_davidson_opts* opts);
+
+/* Solve for the nb lowest eigenpairs at the prepared k-point.
+ *   bands_host   npw x nb (ld npw): in, the starting bands (the reference seeds
+ *                from the stored bands, davidson.hpp:1000-1045; zero columns are
+ *                replaced by lowest-kinetic-energy plane waves, :1047-1101);
+ *                out, the eigenvectors.
+ *   eigenvalues_host  nb: in, stored eigenvalues (all zero = none); out, Ry. */
+int q3b_davidson_solve(q3b_context* ctx, q3b_cplx128* bands_host, double* eigenvalues_host,
+                       int nb, const q3b_davidson_opts* opts, q3b_davidson_stats* stats);
+
+/* Same, with the bands already on the device (npw x nb, ld npw). */
+int q3b_davidson_solve_dev(q3b_context* ctx, q3b_cplx128* bands_dev, double* eigenvalues_host,
+                           int nb, const q3b_davidson_opts* opts, q3b_davidson_stats* stats);
+
+/* ---- dense FP64 subspace kernels (PlanewaveSubspaceManager pieces) ---------- */
+
+/* diagonalize_subspace (subspace_manager/init.hpp:82; subspace/serial.hpp:18-151):
+ * the generalized Hermitian problem H c = eps S c, itype 1, on device matrices
+ * with leading dimension ld; only the upper triangles are read.  Writes n
+ * eigenvalues (ascending) to w_dev and the S-orthonormal eigenvectors to
+ * evec_dev (ld n).  Returns Q3B_ERR_LINALG (LAPACK's info != 0 case) when S is
+ * not positive definite. */
+int q3b_hegv(q3b_context* ctx, int n, const q3b_cplx128* h_dev, const q3b_cplx128* s_dev, int ld,
+             double* w_dev, q3b_cplx128* evec_dev);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,6 +25,19 @@ class Q3BError(RuntimeError):
         self.code = code
 
 
+class ApplyTiming(C.Structure):
+    _fields_ = [("sticks_backward_ms", C.c_double), ("planes_ms", C.c_double),
+                ("sticks_forward_ms", C.c_double), ("projector_overlap_ms", C.c_double),
+                ("d_apply_ms", C.c_double), ("projector_accumulate_ms", C.c_double),
+                ("launches", C.c_int * 6)]
+
+    KERNELS = ("sticks_backward", "planes", "sticks_forward", "projector_overlap", "d_apply",
+               "projector_accumulate")
+
+    def as_dict(self):
+        return {k: (getattr(self, k + "_ms"), self.launches[i]) for i, k in enumerate(self.KERNELS)}
+
+
 class DavidsonOpts(C.Structure):
     _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_int),
                 ("basis_expansion_factor", C.c_int), ("occupied_bands", C.c_int),
@@ -56,6 +69,13 @@ SIGNATURES = {
     "q3b_apply_h": (_i, [_vp, _vp, _vp, _i, _i]),
     "q3b_apply_h_f32": (_i, [_vp, _vp, _vp, _i]),
     "q3b_apply_h_host": (_i, [_vp, _vp, _vp, _i, _i]),
+    "q3b_apply_h_timed": (_i, [_vp, _vp, _vp, _i, _i, C.POINTER(ApplyTiming)]),
+    "q3b_kernel_launches": (C.c_ulonglong, []),
+    "q3b_davidson_default_opts": (None, [C.POINTER(DavidsonOpts)]),
+    "q3b_davidson_solve": (_i, [_vp, _vp, _vp, _i, C.POINTER(DavidsonOpts), C.POINTER(DavidsonStats)]),
+    "q3b_davidson_solve_dev": (_i, [_vp, _vp, _vp, _i, C.POINTER(DavidsonOpts),
+                                    C.POINTER(DavidsonStats)]),
+    "q3b_hegv": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp]),
 }
 
 _lib = None

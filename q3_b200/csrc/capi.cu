@@ -133,4 +133,93 @@ int q3b_apply_h_host(q3b_context* ctx, const q3b_cplx128* psi, q3b_cplx128* hpsi
     });
 }
 
+int q3b_apply_h_timed(q3b_context* ctx, const void* psi, void* hpsi, int nvec, int fp32,
+                      q3b_apply_timing* timing) {
+    return guarded(ctx, [&](Context& c) {
+        if (nvec < 0 || (nvec > 0 && (!psi || !hpsi))) throw q3b::Status(Q3B_ERR_INVALID, "bad vectors");
+        q3b::PhaseTimer tm;
+        tm.st = c.stream;
+        const int npw = c.kp.npw;
+        if (fp32)
+            c.apply_h<float>(static_cast<const float2*>(psi), npw, static_cast<float2*>(hpsi), npw, nvec, &tm);
+        else
+            c.apply_h<double>(static_cast<const double2*>(psi), npw, static_cast<double2*>(hpsi), npw, nvec, &tm);
+        double ms[q3b::PhaseTimer::NCLASS];
+        int cnt[q3b::PhaseTimer::NCLASS];
+        tm.collect(ms, cnt);
+        if (timing) {
+            timing->sticks_backward_ms = ms[0];
+            timing->planes_ms = ms[1];
+            timing->sticks_forward_ms = ms[2];
+            timing->projector_overlap_ms = ms[3];
+            timing->d_apply_ms = ms[4];
+            timing->projector_accumulate_ms = ms[5];
+            for (int i = 0; i < 6; ++i) timing->launches[i] = cnt[i];
+        }
+    });
+}
+
+unsigned long long q3b_kernel_launches(void) { return q3b::launches(); }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- Davidson
+#include "davidson.cuh"
+#include "dense.cuh"
+
+extern "C" {
+
+void q3b_davidson_default_opts(q3b_davidson_opts* o) {
+    if (!o) return;
+    o->tolerance = 1e-2;           // initial_eigenvalue_tolerance (tolerances.hpp:224)
+    o->max_iterations = 20;        // davidson.hpp:1156
+    o->basis_expansion_factor = 2; // davidson.hpp:864
+    o->occupied_bands = 0;         // 0: every band is occupied
+    o->precision = Q3B_FP64;
+    o->refine_sweeps = 6;
+    o->mixed_tolerance = 1e-5;
+}
+
+int q3b_davidson_solve_dev(q3b_context* ctx, q3b_cplx128* bands, double* eig, int nb,
+                           const q3b_davidson_opts* opts, q3b_davidson_stats* stats) {
+    return guarded(ctx, [&](Context& c) {
+        if (!bands || !eig || !opts) throw q3b::Status(Q3B_ERR_INVALID, "null argument");
+        q3b::davidson_solve(c, reinterpret_cast<double2*>(bands), eig, nb, *opts, stats);
+    });
+}
+
+int q3b_davidson_solve(q3b_context* ctx, q3b_cplx128* bands, double* eig, int nb,
+                       const q3b_davidson_opts* opts, q3b_davidson_stats* stats) {
+    return guarded(ctx, [&](Context& c) {
+        if (!bands || !eig || !opts) throw q3b::Status(Q3B_ERR_INVALID, "null argument");
+        c.require_ready();
+        if (nb <= 0 || nb > c.kp.npw) throw q3b::Status(Q3B_ERR_INVALID, "band count must be in [1, npw]");
+        const size_t bytes = (size_t)c.kp.npw * nb * sizeof(double2);
+        c.ws_bands.reserve(&c, bytes);
+        Q3B_CUDA(cudaMemcpyAsync(c.ws_bands.ptr, bands, bytes, cudaMemcpyHostToDevice, c.stream));
+        q3b::davidson_solve(c, c.ws_bands.as<double2>(), eig, nb, *opts, stats);
+        Q3B_CUDA(cudaMemcpyAsync(bands, c.ws_bands.ptr, bytes, cudaMemcpyDeviceToHost, c.stream));
+        Q3B_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int q3b_hegv(q3b_context* ctx, int n, const q3b_cplx128* h, const q3b_cplx128* s, int ld, double* w,
+             q3b_cplx128* evec) {
+    return guarded(ctx, [&](Context& c) {
+        if (n < 0 || ld < n || (n > 0 && (!h || !s || !w || !evec)))
+            throw q3b::Status(Q3B_ERR_INVALID, "bad hegv arguments");
+        if (n == 0) return;
+        c.ws_dense.reserve(&c, q3b::dense::hegv_scratch_bytes(n));
+        q3b::dense::Scratch ws{c.ws_dense.as<char>(), c.ws_dense.bytes, 0};
+        q3b::GemmWorkspace g = c.gemm_ws(q3b::cgemm_workspace_bytes<double>(n, n, n));
+        const int info = q3b::dense::hegv(c.stream, n, reinterpret_cast<const double2*>(h),
+                                          reinterpret_cast<const double2*>(s), ld, w,
+                                          reinterpret_cast<double2*>(evec), n, ws, g);
+        Q3B_CUDA(cudaStreamSynchronize(c.stream));
+        if (info != 0)
+            throw q3b::Status(Q3B_ERR_LINALG, "overlap matrix not positive definite (info " +
+                                                  std::to_string(info) + ")");
+    });
+}
+
 }  // extern "C"

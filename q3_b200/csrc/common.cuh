@@ -75,7 +75,14 @@ struct CudaError : std::runtime_error {
         }                                                                                      \
     } while (0)
 
-#define Q3B_LAUNCH_CHECK() Q3B_CUDA(cudaGetLastError())
+// every kernel launch of the library is followed by Q3B_LAUNCH_CHECK(), which
+// also counts it (q3b_kernel_launches)
+void count_launch();
+#define Q3B_LAUNCH_CHECK()          \
+    do {                            \
+        ::q3b::count_launch();      \
+        Q3B_CUDA(cudaGetLastError()); \
+    } while (0)
 
 inline int ceil_div(long a, long b) { return static_cast<int>((a + b - 1) / b); }
 

@@ -1,5 +1,6 @@
 // q3b context: HBM accounting, potential, k-point plan, H|psi> orchestration.
 #include <cmath>
+#include <atomic>
 #include <cstring>
 
 #include "context.cuh"
@@ -311,26 +312,31 @@ template <typename R> int Context::sticks_chunk(int nvec) const {
 }
 
 template <typename R>
-void Context::apply_h(const cplx_t<R>* psi, long ldpsi, cplx_t<R>* hpsi, long ldh, int nvec) {
+void Context::apply_h(const cplx_t<R>* psi, long ldpsi, cplx_t<R>* hpsi, long ldh, int nvec,
+                      PhaseTimer* tm) {
     using T = cplx_t<R>;
     require_ready();
     if (nvec <= 0) return;
     const LocalPlan<R>& lp = local_plan<R>();
     const int chunk = sticks_chunk<R>(nvec);
     ws_sticks.reserve(this, (size_t)chunk * sticks_bytes_per_band(lp));
-    apply_local<R>(stream, lp, psi, ldpsi, hpsi, ldh, nvec, ws_sticks.as<T>(), chunk);
+    apply_local<R>(stream, lp, psi, ldpsi, hpsi, ldh, nvec, ws_sticks.as<T>(), chunk, tm);
     if (kp.nproj > 0) {
         const size_t pb = (size_t)kp.nproj * nvec * sizeof(T);
         ws_bm.reserve(this, pb);
         ws_bp.reserve(this, pb);
         GemmWorkspace ws = gemm_ws(cgemm_workspace_bytes<R>(kp.nproj, nvec, kp.npw));
         apply_nonlocal<R>(stream, nonlocal<R>(), kp.npw, nvec, psi, ldpsi, hpsi, ldh,
-                          ws_bm.as<T>(), ws_bp.as<T>(), ws);
+                          ws_bm.as<T>(), ws_bp.as<T>(), ws, tm);
     }
 }
 
-template void Context::apply_h<double>(const double2*, long, double2*, long, int);
-template void Context::apply_h<float>(const float2*, long, float2*, long, int);
+template void Context::apply_h<double>(const double2*, long, double2*, long, int, PhaseTimer*);
+template void Context::apply_h<float>(const float2*, long, float2*, long, int, PhaseTimer*);
+
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launches() { return g_launches.load(); }
 template int Context::sticks_chunk<double>(int) const;
 template int Context::sticks_chunk<float>(int) const;
 

@@ -72,6 +72,7 @@ class Context {
 
     // workspaces
     DevBuf ws_sticks, ws_gemm, ws_bm, ws_bp, ws_conv_in, ws_conv_out, ws_host_io;
+    DevBuf ws_solver, ws_dense, ws_bands;
 
     explicit Context(int dev, size_t hbm_budget);
     ~Context();
@@ -87,7 +88,8 @@ class Context {
 
     // H|psi> on device vectors in precision R (the solver's building block)
     template <typename R>
-    void apply_h(const cplx_t<R>* psi, long ldpsi, cplx_t<R>* hpsi, long ldh, int nvec);
+    void apply_h(const cplx_t<R>* psi, long ldpsi, cplx_t<R>* hpsi, long ldh, int nvec,
+                 PhaseTimer* timer = nullptr);
 
     GemmWorkspace gemm_ws(size_t need);
 
@@ -97,6 +99,9 @@ class Context {
 
 // convert an exception into a status code and message
 int fail(q3b_context* c, const std::exception& e);
+
+// kernel launches issued by the library so far
+unsigned long long launches();
 
 }  // namespace q3b
 

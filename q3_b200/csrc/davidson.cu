@@ -1,0 +1,564 @@
+// Device-resident block Davidson.
+//
+// The loop control is the reference's (PlanewaveDavidsonDiagonalizer::solve,
+// davidson.hpp:324-841) with the norm-conserving branches of its serial
+// subspace manager (subspace_manager/serial.hpp): seed from the given bands,
+// fill from lowest-kinetic-energy plane waves; per iteration diagonalise the
+// subspace (generalized, FP64), test |eps_i - eps_i(prev)| < tol, build the
+// TPA-preconditioned corrections of the unconverged bands into the free basis
+// columns, project them out and Cholesky-QR them (MGS fallback), apply H,
+// extend H_sub / S_sub, collapse to nb Ritz vectors when the basis is full.
+//
+// Everything stays on the GPU: V, HV (S|V> aliases V for norm-conserving
+// pseudopotentials), H_sub, S_sub, the eigenvectors.  The host reads only
+// scalars: Cholesky info, the nb eigenvalues, MGS norms.
+//
+// Precision: Davidson<double> is the FP64 solver.  Davidson<float> keeps the
+// vectors and the GEMMs in FP32 and the subspace (H_sub, S_sub, Cholesky,
+// eigensolve) in FP64; the MIXED solve runs it to a loose tolerance, then
+// hands its Ritz vectors to Davidson<double> for the FP64 refinement sweeps.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "davidson.cuh"
+#include "dense.cuh"
+#include "nonlocal.cuh"
+
+namespace q3b {
+namespace {
+
+constexpr double kNormThreshold = 1e-14;    // tolerances.hpp:39
+constexpr double kPrecondFloor = 1e-4;      // tolerances.hpp:50
+constexpr double kEmptyRelax = 5.0;         // tolerances.hpp:65
+constexpr double kEmptyFloor = 1e-5;        // tolerances.hpp:66
+
+inline int grid_for(long n) {
+    long b = (n + 255) / 256;
+    if (b > 148L * 16) b = 148L * 16;
+    return static_cast<int>(b < 1 ? 1 : b);
+}
+
+// R[:, j] /= max(0.5 (1 + x + sqrt(1 + (x-1)^2)), 1e-4), x = KE - eps_j
+// (subspace_manager/serial.hpp:1138-1156)
+template <typename R>
+__global__ void precondition_kernel(int npw, int ncols, const double* __restrict__ ke,
+                                    const double* __restrict__ eps, cplx_t<R>* X) {
+    const long total = (long)npw * ncols;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long)gridDim.x * blockDim.x) {
+        const int g = static_cast<int>(idx % npw);
+        const int j = static_cast<int>(idx / npw);
+        const double x = ke[g] - eps[j];
+        double den = 0.5 * (1.0 + x + sqrt(1.0 + (x - 1.0) * (x - 1.0)));
+        if (den < kPrecondFloor) den = kPrecondFloor;
+        const R inv = static_cast<R>(1.0 / den);
+        cplx_t<R> v = X[idx];
+        v.x *= inv;
+        v.y *= inv;
+        X[idx] = v;
+    }
+}
+
+// out[:, j] = evec[:, idx[j]] (ld n), outneg = -eps_j * out[:, j], in precision R
+template <typename R>
+__global__ void pack_coefficients(int n, int ncols, const double2* __restrict__ evec,
+                                  const int* __restrict__ idx, const double* __restrict__ w,
+                                  cplx_t<R>* out, cplx_t<R>* outneg, double* eps) {
+    const long total = (long)n * ncols;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
+         t += (long)gridDim.x * blockDim.x) {
+        const int r = static_cast<int>(t % n);
+        const int j = static_cast<int>(t / n);
+        const int b = idx[j];
+        const double2 v = evec[r + (long)b * n];
+        const double e = w[b];
+        out[t] = mk(static_cast<R>(v.x), static_cast<R>(v.y));
+        outneg[t] = mk(static_cast<R>(-e * v.x), static_cast<R>(-e * v.y));
+        if (r == 0) eps[j] = e;
+    }
+}
+
+template <typename R>
+__global__ void unit_vectors(int npw, int count, const int* __restrict__ gidx, cplx_t<R>* V) {
+    const long total = (long)npw * count;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
+         t += (long)gridDim.x * blockDim.x) {
+        const int g = static_cast<int>(t % npw);
+        const int j = static_cast<int>(t / npw);
+        V[t] = (g == gidx[j]) ? mk(R(1), R(0)) : mk(R(0), R(0));
+    }
+}
+
+template <typename R>
+__global__ void scale_vector(long n, cplx_t<R>* v, double s) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        cplx_t<R> x = v[i];
+        x.x = static_cast<R>(x.x * s);
+        x.y = static_cast<R>(x.y * s);
+        v[i] = x;
+    }
+}
+
+// dst (double2, ld ldd) = src (R, ld lds), an M x N block
+template <typename R>
+__global__ void widen_block(int M, int N, const cplx_t<R>* __restrict__ src, int lds, double2* dst, int ldd) {
+    const long total = (long)M * N;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
+         t += (long)gridDim.x * blockDim.x) {
+        const int r = static_cast<int>(t % M), c = static_cast<int>(t / M);
+        const cplx_t<R> v = src[r + (long)c * lds];
+        dst[r + (long)c * ldd] = mk((double)v.x, (double)v.y);
+    }
+}
+
+template <typename R>
+__global__ void narrow_block(int M, int N, const double2* __restrict__ src, int lds, cplx_t<R>* dst, int ldd) {
+    const long total = (long)M * N;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
+         t += (long)gridDim.x * blockDim.x) {
+        const int r = static_cast<int>(t % M), c = static_cast<int>(t / M);
+        const double2 v = src[r + (long)c * lds];
+        dst[r + (long)c * ldd] = mk(static_cast<R>(v.x), static_cast<R>(v.y));
+    }
+}
+
+// out[j] = ||X[:, j]||, one block per column, fixed-order reduction
+template <typename R>
+__global__ void column_norms(int npw, const cplx_t<R>* __restrict__ X, double* out) {
+    const cplx_t<R>* x = X + (long)blockIdx.x * npw;
+    double s = 0.0;
+    for (int g = threadIdx.x; g < npw; g += blockDim.x) {
+        const cplx_t<R> v = x[g];
+        s += (double)v.x * v.x + (double)v.y * v.y;
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = sqrt(red[0]);
+}
+
+// carve one device buffer into slices
+struct Carve {
+    char* base;
+    size_t off = 0;
+    template <typename T> T* take(size_t count) {
+        off = (off + 255) & ~size_t(255);
+        T* p = reinterpret_cast<T*>(base + off);
+        off += count * sizeof(T);
+        return p;
+    }
+};
+
+template <typename R> class Davidson {
+  public:
+    using T = cplx_t<R>;
+
+    Davidson(Context& c, int nb, int expansion, DevBuf& mem, DevBuf& dmem)
+        : c_(c), st_(c.stream), npw_(c.kp.npw), nb_(nb) {
+        maxn_ = std::max(std::min(expansion * nb, npw_), nb);  // davidson.hpp:401-404
+        const size_t vecs = (size_t)npw_ * maxn_;
+        const size_t mm = (size_t)maxn_ * maxn_;
+        size_t bytes = 2 * vecs * sizeof(T) + (size_t)npw_ * maxn_ * sizeof(T)  // V, HV, tmp
+                       + 2 * mm * sizeof(double2)                                 // Hs, Ss
+                       + 3 * mm * sizeof(double2)                                 // evec, gram64, uinv64
+                       + 5 * mm * sizeof(T)                                       // evecR, cpack, cneg, coef, uinvR
+                       + 4 * (size_t)maxn_ * sizeof(double) + (size_t)maxn_ * sizeof(int) +
+                       (size_t)npw_ * sizeof(double) + 32 * 256;
+        mem.reserve(&c, bytes);
+        Carve cv{mem.as<char>()};
+        V_ = cv.take<T>(vecs);
+        HV_ = cv.take<T>(vecs);
+        tmp_ = cv.take<T>((size_t)npw_ * maxn_);
+        Hs_ = cv.take<double2>(mm);
+        Ss_ = cv.take<double2>(mm);
+        evec_ = cv.take<double2>(mm);
+        gram_ = cv.take<double2>(mm);
+        uinv_ = cv.take<double2>(mm);
+        evecR_ = cv.take<T>(mm);
+        cpack_ = cv.take<T>(mm);
+        cneg_ = cv.take<T>(mm);
+        coef_ = cv.take<T>(mm);
+        uinvR_ = cv.take<T>(mm);
+        w_ = cv.take<double>(maxn_);
+        eps_ = cv.take<double>(maxn_);
+        norms_ = cv.take<double>(maxn_);
+        idx_ = cv.take<int>(maxn_);
+        ke_ = c.kp.ke64.as<double>();
+        dmem.reserve(&c, dense::hegv_scratch_bytes(maxn_) + dense::potrf_scratch_bytes(maxn_));
+        dscratch_.base = dmem.as<char>();
+        dscratch_.bytes = dmem.bytes;
+        Q3B_CUDA(cudaMemsetAsync(Hs_, 0, mm * sizeof(double2), st_));
+        Q3B_CUDA(cudaMemsetAsync(Ss_, 0, mm * sizeof(double2), st_));
+    }
+
+    int maxn() const { return maxn_; }
+    T* V() { return V_; }
+    T* scratch() { return tmp_; }
+
+    // ------------------------------------------------------------ GEMM
+    void gemm(bool conj, int M, int N, int K, T alpha, const T* A, long lda, const T* B, long ldb, T beta,
+              T* C, long ldc) {
+        GemmWorkspace ws = c_.gemm_ws(conj ? cgemm_workspace_bytes<R>(M, N, K) : 0);
+        cgemm<R>(st_, conj, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, ws);
+    }
+    static T one() { return mk(R(1), R(0)); }
+    static T zero() { return mk(R(0), R(0)); }
+    static T mone() { return mk(R(-1), R(0)); }
+
+    // --------------------------------------- orthogonalize_batch (serial.hpp:41-553)
+    int orthogonalize(int start, int ncand) {
+        if (ncand == 0) return 0;
+        T* Tc = V_ + (size_t)start * npw_;
+        if (start > 0) {
+            gemm(true, start, ncand, npw_, one(), V_, npw_, Tc, npw_, zero(), coef_, start);
+            gemm(false, npw_, ncand, start, mone(), V_, npw_, coef_, start, one(), Tc, npw_);
+        }
+        // Cholesky QR, the Gram matrix and its factor in FP64
+        gemm(true, ncand, ncand, npw_, one(), Tc, npw_, Tc, npw_, zero(), coef_, ncand);
+        widen(ncand, ncand, coef_, ncand, gram_, ncand);
+        dscratch_.used = 0;
+        const int info = dense::potrf(st_, ncand, gram_, ncand, dscratch_);
+        if (info == 0) {
+            // the same scratch still holds the diagonal-block inverses potrf left
+            dscratch_.used = 0;
+            dense::trtri_after_potrf(st_, ncand, gram_, ncand, uinv_, dscratch_);
+            const T* U = narrowed(ncand, ncand, uinv_, ncand, uinvR_);
+            gemm(false, npw_, ncand, ncand, one(), Tc, npw_, U, ncand, zero(), tmp_, npw_);
+            Q3B_CUDA(cudaMemcpyAsync(Tc, tmp_, (size_t)npw_ * ncand * sizeof(T), cudaMemcpyDeviceToDevice, st_));
+            return ncand;
+        }
+        // modified Gram-Schmidt fallback (serial.hpp:370-552)
+        int accepted = 0;
+        for (int cidx = 0; cidx < ncand; ++cidx) {
+            const int src = start + cidx, dst = start + accepted;
+            T* v = V_ + (size_t)dst * npw_;
+            if (dst != src)
+                Q3B_CUDA(cudaMemcpyAsync(v, V_ + (size_t)src * npw_, npw_ * sizeof(T), cudaMemcpyDeviceToDevice, st_));
+            const int nex = dst - start;
+            if (nex > 0) {
+                gemm(true, nex, 1, npw_, one(), Tc, npw_, v, npw_, zero(), coef_, nex);
+                gemm(false, npw_, 1, nex, mone(), Tc, npw_, coef_, nex, one(), v, npw_);
+            }
+            column_norms<R><<<1, 256, 0, st_>>>(npw_, v, norms_);
+            Q3B_LAUNCH_CHECK();
+            double nrm = 0.0;
+            Q3B_CUDA(cudaMemcpyAsync(&nrm, norms_, sizeof(double), cudaMemcpyDeviceToHost, st_));
+            Q3B_CUDA(cudaStreamSynchronize(st_));
+            const double n2 = nrm * nrm;
+            if (n2 > kNormThreshold) {
+                scale_vector<R><<<grid_for(npw_), 256, 0, st_>>>(npw_, v, 1.0 / nrm);
+                Q3B_LAUNCH_CHECK();
+                ++accepted;
+            }
+        }
+        return accepted;
+    }
+
+    // ------------------------------------ update_subspace_matrices (serial.hpp:555-678)
+    void update(int start, int nnew, int total) {
+        if (nnew <= 0) return;
+        const T* Hn = HV_ + (size_t)start * npw_;
+        const T* Sn = V_ + (size_t)start * npw_;
+        if constexpr (std::is_same<R, double>::value) {
+            gemm(true, total, nnew, npw_, one(), V_, npw_, Hn, npw_, zero(), Hs_ + (size_t)start * maxn_, maxn_);
+            gemm(true, total, nnew, npw_, one(), V_, npw_, Sn, npw_, zero(), Ss_ + (size_t)start * maxn_, maxn_);
+        } else {
+            gemm(true, total, nnew, npw_, one(), V_, npw_, Hn, npw_, zero(), coef_, total);
+            widen(total, nnew, coef_, total, Hs_ + (size_t)start * maxn_, maxn_);
+            gemm(true, total, nnew, npw_, one(), V_, npw_, Sn, npw_, zero(), coef_, total);
+            widen(total, nnew, coef_, total, Ss_ + (size_t)start * maxn_, maxn_);
+        }
+    }
+
+    // --------------------------------------- diagonalize_subspace (serial.hpp:680-756)
+    // eigenvalues to w_ (and the first nb to host), eigenvectors (first nvec) to evec_ (ld n)
+    int diagonalize(int n, const double2* H, const double2* S, int ld) {
+        dscratch_.used = 0;
+        const int nvec = std::min(nb_, n);
+        GemmWorkspace gws = c_.gemm_ws(cgemm_workspace_bytes<double>(n, n, n));
+        const int info = dense::hegv(st_, n, H, S, ld, w_, evec_, nvec, dscratch_, gws);
+        if (info == 0) {
+            whost_.assign(n, 0.0);
+            Q3B_CUDA(cudaMemcpyAsync(whost_.data(), w_, n * sizeof(double), cudaMemcpyDeviceToHost, st_));
+            Q3B_CUDA(cudaStreamSynchronize(st_));
+        }
+        return info;
+    }
+
+    // ------------------------------------ build_correction_vectors (serial.hpp:995-1132)
+    int corrections(int basis, const std::vector<int>& bands, int maxcand) {
+        int ncand = std::min<int>(static_cast<int>(bands.size()), maxcand);
+        if (ncand <= 0) return 0;
+        Q3B_CUDA(cudaMemcpyAsync(idx_, bands.data(), ncand * sizeof(int), cudaMemcpyHostToDevice, st_));
+        pack_coefficients<R><<<grid_for((long)basis * ncand), 256, 0, st_>>>(basis, ncand, evec_, idx_, w_,
+                                                                             cpack_, cneg_, eps_);
+        Q3B_LAUNCH_CHECK();
+        T* Rc = V_ + (size_t)basis * npw_;
+        gemm(false, npw_, ncand, basis, one(), V_, npw_, cneg_, basis, zero(), Rc, npw_);   // -(SV)c eps
+        gemm(false, npw_, ncand, basis, one(), HV_, npw_, cpack_, basis, one(), Rc, npw_);  // + (HV)c
+        precondition_kernel<R><<<grid_for((long)npw_ * ncand), 256, 0, st_>>>(npw_, ncand, ke_, eps_, Rc);
+        Q3B_LAUNCH_CHECK();
+        return ncand;
+    }
+
+    // rotate V and HV onto the first nb eigenvectors of the last diagonalisation
+    void rotate(int basis) {
+        const T* C = narrowed(basis, nb_, evec_, basis, evecR_);
+        const size_t bytes = (size_t)npw_ * nb_ * sizeof(T);
+        gemm(false, npw_, nb_, basis, one(), V_, npw_, C, basis, zero(), tmp_, npw_);
+        Q3B_CUDA(cudaMemcpyAsync(V_, tmp_, bytes, cudaMemcpyDeviceToDevice, st_));
+        gemm(false, npw_, nb_, basis, one(), HV_, npw_, C, basis, zero(), tmp_, npw_);
+        Q3B_CUDA(cudaMemcpyAsync(HV_, tmp_, bytes, cudaMemcpyDeviceToDevice, st_));
+    }
+
+    // --------------------------------------- collapse_subspace (serial.hpp:825-945)
+    int collapse(int basis, bool from_held) {
+        int info = -1;
+        if (from_held) info = diagonalize(basis, Hs_, Ss_, maxn_);
+        if (info != 0) {
+            // rebuild the subspace from the vectors
+            T* h = coef_;
+            gemm(true, basis, basis, npw_, one(), V_, npw_, HV_, npw_, zero(), h, basis);
+            widen(basis, basis, h, basis, gram_, basis);
+            gemm(true, basis, basis, npw_, one(), V_, npw_, V_, npw_, zero(), h, basis);
+            widen(basis, basis, h, basis, uinv_, basis);
+            info = diagonalize(basis, gram_, uinv_, basis);
+            if (info != 0) throw Status(Q3B_ERR_LINALG, "subspace eigensolver failed in the collapse");
+        }
+        rotate(basis);
+        const size_t mm = (size_t)maxn_ * maxn_;
+        Q3B_CUDA(cudaMemsetAsync(Hs_, 0, mm * sizeof(double2), st_));
+        Q3B_CUDA(cudaMemsetAsync(Ss_, 0, mm * sizeof(double2), st_));
+        update(0, nb_, nb_);
+        return nb_;
+    }
+
+    // psi = V c[:, :nb] into out (npw x nb), the FP64 residual norms ||HVc - eps Vc||
+    void extract(int basis, T* out, double* resid_max) {
+        const T* C = narrowed(basis, nb_, evec_, basis, evecR_);
+        gemm(false, npw_, nb_, basis, one(), V_, npw_, C, basis, zero(), out, npw_);
+        if (resid_max) {
+            std::vector<int> all(nb_);
+            std::iota(all.begin(), all.end(), 0);
+            Q3B_CUDA(cudaMemcpyAsync(idx_, all.data(), nb_ * sizeof(int), cudaMemcpyHostToDevice, st_));
+            pack_coefficients<R><<<grid_for((long)basis * nb_), 256, 0, st_>>>(basis, nb_, evec_, idx_, w_,
+                                                                               cpack_, cneg_, eps_);
+            Q3B_LAUNCH_CHECK();
+            gemm(false, npw_, nb_, basis, one(), V_, npw_, cneg_, basis, zero(), tmp_, npw_);
+            gemm(false, npw_, nb_, basis, one(), HV_, npw_, cpack_, basis, one(), tmp_, npw_);
+            column_norms<R><<<nb_, 256, 0, st_>>>(npw_, tmp_, norms_);
+            Q3B_LAUNCH_CHECK();
+            std::vector<double> h(nb_);
+            Q3B_CUDA(cudaMemcpyAsync(h.data(), norms_, nb_ * sizeof(double), cudaMemcpyDeviceToHost, st_));
+            Q3B_CUDA(cudaStreamSynchronize(st_));
+            *resid_max = *std::max_element(h.begin(), h.end());
+        }
+    }
+
+    void apply(int first, int count) {
+        if (count <= 0) return;
+        c_.apply_h<R>(V_ + (size_t)first * npw_, npw_, HV_ + (size_t)first * npw_, npw_, count);
+        happly_ += count;
+    }
+
+    std::vector<double> subspace_diagonal(int n) {
+        std::vector<double2> d(n);
+        Q3B_CUDA(cudaMemcpy2DAsync(d.data(), sizeof(double2), Hs_, (maxn_ + 1) * sizeof(double2),
+                                   sizeof(double2), n, cudaMemcpyDeviceToHost, st_));
+        Q3B_CUDA(cudaStreamSynchronize(st_));
+        std::vector<double> r(n);
+        for (int i = 0; i < n; ++i) r[i] = d[i].x;
+        return r;
+    }
+
+    // The solve of davidson.hpp:324-841 on bands already in V[:, :nb].
+    // Returns the eigenvalues; the eigenvectors go to `out`.
+    struct Result {
+        std::vector<double> eig;
+        int iterations = 0, unconverged = 0, collapses = 0;
+        double resid = 0.0;
+    };
+
+    Result solve(int seeded, const std::vector<double>& stored, double tol, int max_it, int occupied,
+                 T* out, bool want_resid) {
+        Result res;
+        int basis = orthogonalize(0, seeded);                            // :1000-1045
+        apply(0, basis);
+        if (basis < nb_) {                                                // :1047-1101
+            const std::vector<double>& ke = c_.kp.ke_host;
+            std::vector<int> order(npw_);
+            std::iota(order.begin(), order.end(), 0);
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return ke[a] < ke[b]; });
+            const int start = basis;
+            std::vector<int> gsel;
+            for (int band = start; band < nb_; ++band) gsel.push_back(order[band]);
+            const int ncand = static_cast<int>(gsel.size());
+            Q3B_CUDA(cudaMemcpyAsync(idx_, gsel.data(), ncand * sizeof(int), cudaMemcpyHostToDevice, st_));
+            unit_vectors<R><<<grid_for((long)npw_ * ncand), 256, 0, st_>>>(npw_, ncand, idx_,
+                                                                           V_ + (size_t)basis * npw_);
+            Q3B_LAUNCH_CHECK();
+            basis += orthogonalize(basis, ncand);
+            apply(start, basis - start);
+        }
+        if (basis < nb_)
+            throw Status(Q3B_ERR_LINALG, "could not build " + std::to_string(nb_) +
+                                             " independent starting vectors");
+        update(0, basis, basis);                                          // :459-469
+        std::vector<double> prev(nb_, 0.0);
+        bool have_stored = false;
+        for (double e : stored) have_stored = have_stored || e != 0.0;
+        if (have_stored) {
+            prev = stored;                                                // :483-487
+        } else {
+            std::vector<double> dg = subspace_diagonal(std::min(nb_, basis));
+            std::copy(dg.begin(), dg.end(), prev.begin());                // :488-494
+        }
+        const double empty_tol = std::max(kEmptyRelax * tol, kEmptyFloor);
+        for (int it = 0; it < max_it; ++it) {                            // :498
+            int info = diagonalize(basis, Hs_, Ss_, maxn_);
+            if (info != 0 && basis > nb_) {                               // :521-590
+                basis = collapse(basis, false);
+                ++res.collapses;
+                info = diagonalize(basis, Hs_, Ss_, maxn_);
+                if (info != 0) {
+                    whost_.assign(std::max(basis, nb_), 0.0);
+                    std::copy(prev.begin(), prev.end(), whost_.begin());
+                }
+            } else if (info != 0) {
+                throw Status(Q3B_ERR_LINALG, "subspace eigensolver failed");
+            }
+            ++res.iterations;
+            std::vector<int> unconv;
+            for (int b = 0; b < nb_; ++b) {                               // :615-629
+                const double change = std::fabs(whost_[b] - prev[b]);
+                const double tb = b < occupied ? tol : empty_tol;
+                if (!(it != 0 && change < tb)) unconv.push_back(b);
+            }
+            res.unconverged = static_cast<int>(unconv.size());
+            if (unconv.empty()) {                                         // :649-668
+                extract(basis, out, want_resid ? &res.resid : nullptr);
+                res.eig.assign(whost_.begin(), whost_.begin() + nb_);
+                return res;
+            }
+            const int ncand = corrections(basis, unconv, maxn_ - basis);  // :689-703
+            const int acc = orthogonalize(basis, ncand);                  // :705-712
+            apply(basis, acc);                                            // :728-738
+            const int old = basis;
+            basis += acc;
+            if (acc > 0) update(old, acc, basis);                         // :743-760
+            if (basis >= maxn_) {                                         // :763-808
+                basis = collapse(basis, true);
+                ++res.collapses;
+            }
+            for (int b = 0; b < nb_; ++b) prev[b] = whost_[b];
+        }
+        const int info = diagonalize(basis, Hs_, Ss_, maxn_);             // :816-840
+        if (info != 0) throw Status(Q3B_ERR_LINALG, "subspace eigensolver failed at exit");
+        extract(basis, out, want_resid ? &res.resid : nullptr);
+        res.eig.assign(whost_.begin(), whost_.begin() + nb_);
+        return res;
+    }
+
+    int happly() const { return happly_; }
+
+  private:
+    void widen(int M, int N, const T* src, int lds, double2* dst, int ldd) {
+        widen_block<R><<<grid_for((long)M * N), 256, 0, st_>>>(M, N, src, lds, dst, ldd);
+        Q3B_LAUNCH_CHECK();
+    }
+    const T* narrowed(int M, int N, const double2* src, int lds, T* buf) {
+        if constexpr (std::is_same<R, double>::value) {
+            (void)M;
+            (void)N;
+            (void)lds;
+            (void)buf;
+            return src;
+        } else {
+            narrow_block<R><<<grid_for((long)M * N), 256, 0, st_>>>(M, N, src, lds, buf, M);
+            Q3B_LAUNCH_CHECK();
+            return buf;
+        }
+    }
+
+    Context& c_;
+    cudaStream_t st_;
+    int npw_, nb_, maxn_ = 0;
+    int happly_ = 0;
+    T *V_, *HV_, *tmp_, *evecR_, *cpack_, *cneg_, *coef_, *uinvR_;
+    double2 *Hs_, *Ss_, *evec_, *gram_, *uinv_;
+    double *w_, *eps_, *norms_;
+    int* idx_;
+    const double* ke_;
+    dense::Scratch dscratch_;
+    std::vector<double> whost_;
+};
+
+}  // namespace
+
+void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, const q3b_davidson_opts& o,
+                    q3b_davidson_stats* stats) {
+    c.require_ready();
+    const int npw = c.kp.npw;
+    if (nb <= 0 || nb > npw) throw Status(Q3B_ERR_INVALID, "band count must be in [1, npw]");
+    if (o.basis_expansion_factor < 2) throw Status(Q3B_ERR_INVALID, "basis_expansion_factor must be >= 2");
+    if (!(o.tolerance > 0.0)) throw Status(Q3B_ERR_INVALID, "tolerance must be positive");
+    const auto t0 = std::chrono::steady_clock::now();
+    const int occupied = o.occupied_bands > 0 ? std::min(o.occupied_bands, nb) : nb;
+    std::vector<double> stored(eig_host, eig_host + nb);
+    q3b_davidson_stats s{};
+    const size_t band_bytes = (size_t)npw * nb * sizeof(double2);
+    if (o.precision == Q3B_FP64) {
+        Davidson<double> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
+        Q3B_CUDA(cudaMemcpyAsync(dv.V(), bands_dev, band_bytes, cudaMemcpyDeviceToDevice, c.stream));
+        auto r = dv.solve(nb, stored, o.tolerance, std::max(1, o.max_iterations), occupied, bands_dev, true);
+        std::copy(r.eig.begin(), r.eig.end(), eig_host);
+        s.iterations = s.fp64_iterations = r.iterations;
+        s.h_applications = dv.happly();
+        s.unconverged = r.unconverged;
+        s.collapses = r.collapses;
+        s.max_residual_norm = r.resid;
+    } else if (o.precision == Q3B_MIXED) {
+        // FP32 phase to the loose tolerance
+        std::vector<double> eig32;
+        int it32 = 0, h32 = 0, col32 = 0;
+        {
+            Davidson<float> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
+            convert<double, float>(c.stream, (long)npw * nb, bands_dev, dv.V());
+            const double tol32 = o.mixed_tolerance > 0.0 ? o.mixed_tolerance : 1e-5;
+            auto r = dv.solve(nb, stored, std::max(tol32, o.tolerance), std::max(1, o.max_iterations),
+                              occupied, dv.scratch(), false);
+            // widen the FP32 Ritz vectors into the caller's bands
+            convert<float, double>(c.stream, (long)npw * nb, dv.scratch(), bands_dev);
+            eig32 = r.eig;
+            it32 = r.iterations;
+            h32 = dv.happly();
+            col32 = r.collapses;
+        }
+        // FP64 refinement sweeps from the FP32 Ritz pairs
+        Davidson<double> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
+        Q3B_CUDA(cudaMemcpyAsync(dv.V(), bands_dev, band_bytes, cudaMemcpyDeviceToDevice, c.stream));
+        const int sweeps = o.refine_sweeps > 0 ? o.refine_sweeps : 6;
+        auto r = dv.solve(nb, eig32, o.tolerance, sweeps, occupied, bands_dev, true);
+        std::copy(r.eig.begin(), r.eig.end(), eig_host);
+        s.iterations = it32 + r.iterations;
+        s.fp64_iterations = r.iterations;
+        s.h_applications = h32 + dv.happly();
+        s.unconverged = r.unconverged;
+        s.collapses = col32 + r.collapses;
+        s.max_residual_norm = r.resid;
+    } else {
+        throw Status(Q3B_ERR_INVALID, "unknown precision");
+    }
+    Q3B_CUDA(cudaStreamSynchronize(c.stream));
+    s.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (stats) *stats = s;
+}
+
+}  // namespace q3b

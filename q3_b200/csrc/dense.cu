@@ -1,0 +1,718 @@
+// FP64 dense kernels for the Davidson subspace; see dense.cuh.
+//
+// potrf : blocked right-looking upper Cholesky (32x32 blocks): a diagonal
+//         block factor + its triangular inverse, a panel solve and a trailing
+//         update per block step.
+// trtri : U^{-1} block column by block column, each a set of independent
+//         block products.
+// hegv  : H c = w S c reduced to C = U^{-H} H U^{-1} with S = U^H U, as
+//         zhegv does (subspace/serial.hpp:18-151 calls zhegv itype 1), solved
+//         by heev, back-transformed c = U^{-1} z.
+// heev  : Householder tridiagonalisation in one cooperative kernel (two grid
+//         barriers per column, each wait bounded), the complex subdiagonal
+//         made real by a diagonal phase, eigenvalues by multisection on
+//         Sturm counts (one warp per eigenvalue), eigenvectors by inverse
+//         iteration with Gram-Schmidt inside clusters of close eigenvalues,
+//         then the reflectors applied back (one warp per vector).
+#include <cmath>
+#include <vector>
+
+#include "context.cuh"
+#include "dense.cuh"
+#include "q3b.h"
+
+namespace q3b {
+namespace dense {
+namespace {
+
+constexpr int NB = 32;
+
+__device__ __forceinline__ int vload(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
+
+// ------------------------------------------------------------------ potrf
+__global__ void __launch_bounds__(256)
+potrf_diag(int n, int k, double2* A, int lda, double2* dinv, int* info) {
+    if (vload(info)) return;
+    __shared__ double2 a[NB][NB + 1];  // a[c][r] = element (r, c)
+    __shared__ double2 x[NB][NB + 1];
+    __shared__ int bad;
+    const int r0 = k * NB;
+    const int bs = min(NB, n - r0);
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+        const int r = idx % NB, c = idx / NB;
+        double2 v = (r == c) ? mk(1.0, 0.0) : mk(0.0, 0.0);
+        if (r < bs && c < bs) v = A[(r0 + r) + (long)(r0 + c) * lda];
+        a[c][r] = v;
+        x[c][r] = mk(0.0, 0.0);
+    }
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    for (int j = 0; j < NB; ++j) {
+        if (tid == 0) {
+            double piv = a[j][j].x;
+            if (!(piv > 0.0)) {
+                if (!bad && j < bs) bad = r0 + j + 1;
+                piv = 1.0;
+            }
+            a[j][j] = mk(sqrt(piv), 0.0);
+        }
+        __syncthreads();
+        if (tid > j && tid < NB) {
+            const double u = a[j][j].x;
+            a[tid][j] = mk(a[tid][j].x / u, a[tid][j].y / u);
+        }
+        __syncthreads();
+        for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+            const int r = idx % NB, c = idx / NB;
+            if (r > j && c >= r) a[c][r] = a[c][r] - cmulc(a[r][j], a[c][j]);
+        }
+        __syncthreads();
+    }
+    // X = U^{-1}: column c by thread c
+    if (tid < NB) {
+        const int c = tid;
+        for (int r = c; r >= 0; --r) {
+            double2 s = (r == c) ? mk(1.0, 0.0) : mk(0.0, 0.0);
+            for (int t = r + 1; t <= c; ++t) s = s - cmul(a[t][r], x[c][t]);
+            const double u = a[r][r].x;
+            x[c][r] = mk(s.x / u, s.y / u);
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+        const int r = idx % NB, c = idx / NB;
+        if (r < bs && c < bs && r <= c) A[(r0 + r) + (long)(r0 + c) * lda] = a[c][r];
+        dinv[(long)k * NB * NB + r + c * NB] = x[c][r];
+    }
+    if (tid == 0 && bad) atomicCAS(info, 0, bad);
+}
+
+// U(k, j) = U_kk^{-H} G(k, j) for every block column j > k
+__global__ void __launch_bounds__(256)
+potrf_panel(int n, int k, double2* A, int lda, const double2* dinv, const int* info) {
+    if (vload(info)) return;
+    __shared__ double2 xk[NB][NB + 1];  // xk[c][r] = Xk(r, c)
+    __shared__ double2 g[NB][NB + 1];   // g[c][t] = G(k_t, j_c)
+    const int j = k + 1 + blockIdx.x;
+    const int r0 = k * NB, c0 = j * NB;
+    const int bsk = min(NB, n - r0), bsj = min(NB, n - c0);
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+        const int r = idx % NB, c = idx / NB;
+        xk[c][r] = dinv[(long)k * NB * NB + r + c * NB];
+        g[c][r] = (r < bsk && c < bsj) ? A[(r0 + r) + (long)(c0 + c) * lda] : mk(0.0, 0.0);
+    }
+    __syncthreads();
+    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+        const int r = idx % NB, c = idx / NB;
+        double2 s = mk(0.0, 0.0);
+        for (int t = 0; t <= r; ++t) s = s + cmulc(xk[r][t], g[c][t]);
+        if (r < bsk && c < bsj) A[(r0 + r) + (long)(c0 + c) * lda] = s;
+    }
+}
+
+// G(i, j) -= U(k, i)^H U(k, j) for k < i <= j
+__global__ void __launch_bounds__(256) potrf_update(int n, int k, double2* A, int lda, const int* info) {
+    if (vload(info)) return;
+    const int i = k + 1 + blockIdx.x, j = k + 1 + blockIdx.y;
+    if (i > j) return;
+    __shared__ double2 ui[NB][NB + 1];  // ui[r][t] = U(k_t, i_r)
+    __shared__ double2 uj[NB][NB + 1];  // uj[c][t] = U(k_t, j_c)
+    const int r0 = k * NB, ci = i * NB, cj = j * NB;
+    const int bsk = min(NB, n - r0), bsi = min(NB, n - ci), bsj = min(NB, n - cj);
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+        const int t = idx % NB, c = idx / NB;
+        ui[c][t] = (t < bsk && c < bsi) ? A[(r0 + t) + (long)(ci + c) * lda] : mk(0.0, 0.0);
+        uj[c][t] = (t < bsk && c < bsj) ? A[(r0 + t) + (long)(cj + c) * lda] : mk(0.0, 0.0);
+    }
+    __syncthreads();
+    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+        const int r = idx % NB, c = idx / NB;
+        if (r >= bsi || c >= bsj) continue;
+        double2 s = mk(0.0, 0.0);
+        for (int t = 0; t < NB; ++t) s = s + cmulc(ui[r][t], uj[c][t]);
+        double2* p = A + (ci + r) + (long)(cj + c) * lda;
+        *p = *p - s;
+    }
+}
+
+// ------------------------------------------------------------------ trtri
+__global__ void trtri_diag(int n, const double2* dinv, double2* U) {
+    const int k = blockIdx.x;
+    const int r0 = k * NB, bs = min(NB, n - r0);
+    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+        const int r = idx % NB, c = idx / NB;
+        if (r < bs && c < bs) U[(r0 + r) + (long)(r0 + c) * n] = dinv[(long)k * NB * NB + r + c * NB];
+    }
+}
+
+// Uinv(i, j) = -[sum_{t=i}^{j-1} Uinv(i, t) U(t, j)] X_j for all i < j
+__global__ void __launch_bounds__(256)
+trtri_col(int n, int j, const double2* A, int lda, const double2* dinv, double2* Ui) {
+    const int i = blockIdx.x;
+    __shared__ double2 p[NB][NB + 1];  // p[q][r] = Uinv(i_r, t_q)
+    __shared__ double2 u[NB][NB + 1];  // u[c][q] = U(t_q, j_c)
+    const int tid = threadIdx.x;
+    const int bsi = min(NB, n - i * NB), bsj = min(NB, n - j * NB);
+    double2 acc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = mk(0.0, 0.0);
+    for (int t = i; t < j; ++t) {
+        const int bst = min(NB, n - t * NB);
+        __syncthreads();
+        for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+            const int r = idx % NB, q = idx / NB;
+            p[q][r] = (r < bsi && q < bst) ? Ui[(i * NB + r) + (long)(t * NB + q) * n] : mk(0.0, 0.0);
+            u[r][q] = (q < bst && r < bsj) ? A[(t * NB + q) + (long)(j * NB + r) * lda] : mk(0.0, 0.0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const int idx = tid + s * 256;
+            const int r = idx % NB, c = idx / NB;
+            double2 a = acc[s];
+            for (int q = 0; q < NB; ++q) a = a + cmul(p[q][r], u[c][q]);
+            acc[s] = a;
+        }
+    }
+    __syncthreads();
+    // p <- acc, u <- X_j
+    for (int s = 0; s < 4; ++s) {
+        const int idx = tid + s * 256;
+        const int r = idx % NB, c = idx / NB;
+        p[c][r] = acc[s];
+        u[c][r] = dinv[(long)j * NB * NB + r + c * NB];
+    }
+    __syncthreads();
+    for (int s = 0; s < 4; ++s) {
+        const int idx = tid + s * 256;
+        const int r = idx % NB, c = idx / NB;
+        double2 a = mk(0.0, 0.0);
+        for (int q = 0; q < NB; ++q) a = a + cmul(p[q][r], u[c][q]);
+        if (r < bsi && c < bsj) Ui[(i * NB + r) + (long)(j * NB + c) * n] = mk(-a.x, -a.y);
+    }
+}
+
+// ------------------------------------------------------------------ helpers
+// dst (n x n, ld n) = full Hermitian matrix from the upper triangle of src (ld lds)
+__global__ void hermitian_from_upper(int n, const double2* src, int lds, double2* dst) {
+    const long total = (long)n * n;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long)gridDim.x * blockDim.x) {
+        const int r = static_cast<int>(idx % n), c = static_cast<int>(idx / n);
+        double2 v;
+        if (r < c) v = src[r + (long)c * lds];
+        else if (r > c) v = conj2(src[c + (long)r * lds]);
+        else v = mk(src[r + (long)c * lds].x, 0.0);
+        dst[idx] = v;
+    }
+}
+
+__global__ void copy_matrix(int n, const double2* src, int lds, double2* dst, int ldd) {
+    const long total = (long)n * n;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long)gridDim.x * blockDim.x) {
+        const int r = static_cast<int>(idx % n), c = static_cast<int>(idx / n);
+        dst[r + (long)c * ldd] = src[r + (long)c * lds];
+    }
+}
+
+inline int grid_for(long n) {
+    long b = (n + 255) / 256;
+    if (b > 148L * 8) b = 148L * 8;
+    return static_cast<int>(b < 1 ? 1 : b);
+}
+
+// ------------------------------------------------------------ grid barrier
+// Arrival counter + generation word; every wait is bounded (about 2 s of
+// clock), after which the kernel records an error and all blocks leave.
+__device__ __forceinline__ bool grid_sync(unsigned* bar, unsigned nblocks, int* err) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = bar + 1;
+        const unsigned gen = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u);
+        int ok = 1;
+        if (arrived == nblocks - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            const long long t0 = clock64();
+            while (*vgen == gen) {
+                if (vload(err)) {
+                    ok = 0;
+                    break;
+                }
+                if (clock64() - t0 > (1LL << 32)) {
+                    atomicExch(err, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+__device__ __forceinline__ double2 warp_sum(double2 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------------ hetrd
+// A (n x n, ld n, full Hermitian) reduced to tridiagonal form by reflectors
+// H_k = I - tau_k v_k v_k^H acting on rows/columns k+1..n-1:
+//   d[k] = A_kk, e[k] = T(k+1, k) (complex), v_k in Vh[:, k] (rows k+1..), tau[k].
+// Column i of the trailing matrix belongs to warp (i mod total warps).
+// Data other blocks write is read with ld.global.cg (L2), never from L1.
+__global__ void __launch_bounds__(256)
+hetrd_coop(int n, double2* A, double* d, double2* e, double2* Vh, double* tau, double2* pbuf,
+           double2* partial, unsigned* bar, int* err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double2* sv = reinterpret_cast<double2*>(smem);
+    double2* sw = sv + n;
+    __shared__ double red[8];
+    __shared__ double2 redc[8];
+    __shared__ double s_tau;
+    __shared__ double2 s_alpha, s_x0;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int gw = blockIdx.x * 8 + warp;
+    const int nw = gridDim.x * 8;
+    for (int k = 0; k + 1 < n; ++k) {
+        const int m = n - k - 1;
+        // x = A[k+1:, k]
+        double part = 0.0;
+        for (int j = tid; j < m; j += blockDim.x) {
+            const double2 x = __ldcg(&A[(k + 1 + j) + (long)k * n]);
+            sv[j] = x;
+            if (j > 0) part += x.x * x.x + x.y * x.y;
+        }
+        part = warp_sum(part);
+        if (lane == 0) red[warp] = part;
+        __syncthreads();
+        if (tid == 0) {
+            double sigma = 0.0;
+            for (int q = 0; q < 8; ++q) sigma += red[q];
+            const double2 x0 = sv[0];
+            double t = 0.0;
+            double2 alpha = x0;
+            if (m > 1 && sigma > 0.0) {
+                const double ax0 = hypot(x0.x, x0.y);
+                const double nrm = sqrt(sigma + ax0 * ax0);
+                alpha = ax0 > 0.0 ? mk(-nrm * x0.x / ax0, -nrm * x0.y / ax0) : mk(-nrm, 0.0);
+                const double2 v0 = x0 - alpha;
+                t = 2.0 / (sigma + v0.x * v0.x + v0.y * v0.y);
+                sv[0] = v0;
+            }
+            s_tau = t;
+            s_alpha = alpha;
+            s_x0 = x0;
+            if (blockIdx.x == 0) {
+                d[k] = __ldcg(&A[k + (long)k * n]).x;
+                e[k] = alpha;
+                tau[k] = t;
+            }
+        }
+        __syncthreads();
+        const double tk = s_tau;
+        if (blockIdx.x == 0) {
+            for (int j = tid; j < m; j += blockDim.x) Vh[(k + 1 + j) + (long)k * n] = tk != 0.0 ? sv[j] : mk(0.0, 0.0);
+        }
+        // p_i = tau * (column i)^H v for owned columns; partial v^H p
+        double2 acc = mk(0.0, 0.0);
+        if (tk != 0.0) {
+            for (int i = k + 1 + ((gw - (k + 1)) % nw + nw) % nw; i < n; i += nw) {
+                double2 s = mk(0.0, 0.0);
+                const double2* col = A + (long)i * n + (k + 1);
+                for (int j = lane; j < m; j += 32) s = s + cmulc(__ldcg(&col[j]), sv[j]);
+                s = warp_sum(s);
+                const double2 p = mk(tk * s.x, tk * s.y);
+                if (lane == 0) pbuf[i] = p;
+                acc = acc + cmulc(sv[i - k - 1], p);
+            }
+        }
+        if (lane == 0) redc[warp] = acc;
+        __syncthreads();
+        if (tid == 0) {
+            double2 s = mk(0.0, 0.0);
+            for (int q = 0; q < 8; ++q) s = s + redc[q];
+            partial[blockIdx.x] = s;
+        }
+        if (!grid_sync(bar, gridDim.x, err)) return;
+        if (tk != 0.0) {
+            if (tid == 0) {
+                double2 s = mk(0.0, 0.0);
+                for (int b = 0; b < (int)gridDim.x; ++b) s = s + __ldcg(&partial[b]);
+                redc[0] = s;
+            }
+            __syncthreads();
+            const double half = 0.5 * tk * redc[0].x;  // v^H p is real
+            for (int j = tid; j < m; j += blockDim.x) {
+                const double2 p = __ldcg(&pbuf[k + 1 + j]);
+                sw[j] = mk(p.x - half * sv[j].x, p.y - half * sv[j].y);
+            }
+            __syncthreads();
+            for (int i = k + 1 + ((gw - (k + 1)) % nw + nw) % nw; i < n; i += nw) {
+                const double2 vi = sv[i - k - 1], wi = sw[i - k - 1];
+                double2* col = A + (long)i * n + (k + 1);
+                for (int j = lane; j < m; j += 32) {
+                    // A[j, i] -= v_j conj(w_i) + w_j conj(v_i)
+                    const double2 a = __ldcg(&col[j]);
+                    const double2 u = cmul(sv[j], conj2(wi)) + cmul(sw[j], conj2(vi));
+                    col[j] = a - u;
+                }
+            }
+        }
+        if (!grid_sync(bar, gridDim.x, err)) return;
+    }
+    if (blockIdx.x == 0 && tid == 0) {
+        d[n - 1] = __ldcg(&A[(n - 1) + (long)(n - 1) * n]).x;
+        e[n - 1] = mk(0.0, 0.0);
+        tau[n - 1] = 0.0;
+    }
+}
+
+// |e|, e^2, the phases delta_{k+1} = delta_k e_k/|e_k| and Gershgorin bounds
+__global__ void tridiag_prep(int n, const double* d, const double2* e, double* ea, double* e2,
+                             double2* phase, double* bounds) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double2 ph = mk(1.0, 0.0);
+    double lo = 1e300, hi = -1e300;
+    for (int k = 0; k < n; ++k) {
+        phase[k] = ph;
+        const double a = (k + 1 < n) ? hypot(e[k].x, e[k].y) : 0.0;
+        if (k + 1 < n) {
+            ea[k] = a;
+            e2[k] = a * a;
+            if (a > 0.0) ph = cmul(ph, mk(e[k].x / a, e[k].y / a));
+        }
+        const double left = (k > 0) ? ea[k - 1] : 0.0;
+        lo = fmin(lo, d[k] - left - a);
+        hi = fmax(hi, d[k] + left + a);
+    }
+    const double scale = fmax(fabs(lo), fabs(hi));
+    bounds[0] = lo - 4.0 * 2.220446049250313e-16 * scale - 1e-300;
+    bounds[1] = hi + 4.0 * 2.220446049250313e-16 * scale + 1e-300;
+    bounds[2] = scale;
+}
+
+// number of eigenvalues of the real tridiagonal (d, e2) below x
+__device__ __forceinline__ int sturm_count(int n, const double* d, const double* e2, double x, double pivmin) {
+    int c = 0;
+    double q = d[0] - x;
+    if (fabs(q) < pivmin) q = -pivmin;
+    c += q < 0.0;
+    for (int k = 1; k < n; ++k) {
+        q = (d[k] - x) - e2[k - 1] / q;
+        if (fabs(q) < pivmin) q = -pivmin;
+        c += q < 0.0;
+    }
+    return c;
+}
+
+// one warp per eigenvalue: 32-point multisection of [lo, hi] on Sturm counts
+__global__ void tridiag_multisect(int n, const double* d, const double* e2, const double* bounds, double* w) {
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n) return;
+    double a = bounds[0], b = bounds[1];
+    const double scale = bounds[2];
+    const double pivmin = fmax(1e-290, 1e-300 * scale * scale);
+    const double tol = 4.0 * 2.220446049250313e-16 * fmax(scale, 1e-300);
+    for (int it = 0; it < 64 && (b - a) > tol; ++it) {
+        const double x = a + (b - a) * (lane + 1) / 33.0;
+        const int cnt = sturm_count(n, d, e2, x, pivmin);
+        // first lane whose point has more than i eigenvalues below it
+        const unsigned above = __ballot_sync(0xffffffffu, cnt > i);
+        const int l = above ? __ffs(above) - 1 : 32;
+        const double na = (l == 0) ? a : a + (b - a) * l / 33.0;
+        const double nb = (l == 32) ? b : a + (b - a) * (l + 1) / 33.0;
+        a = na;
+        b = nb;
+    }
+    if (lane == 0) w[i] = 0.5 * (a + b);
+}
+
+// Inverse iteration, one thread per cluster of close eigenvalues (gap below
+// 1e-3 * ||T||, as LAPACK's dstein groups them); Gram-Schmidt inside a cluster.
+__global__ void tridiag_invit(int n, const double* d, const double* ea, const double* w,
+                              const double* bounds, int nvec, double* Y, double* work) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nvec) return;
+    const double scale = fmax(bounds[2], 1e-300);
+    const double ortol = 1e-3 * scale;
+    if (i > 0 && w[i] - w[i - 1] <= ortol) return;
+    int jend = i + 1;
+    while (jend < nvec && w[jend] - w[jend - 1] <= ortol) ++jend;
+    double* DL = work + (size_t)i * 5 * n;
+    double* D = DL + n;
+    double* DU = D + n;
+    double* DU2 = DU + n;
+    int* piv = reinterpret_cast<int*>(DU2 + n);
+    const double eps = 2.220446049250313e-16;
+    const double tiny = eps * scale;
+    double lam_prev = 0.0;
+    for (int j = i; j < jend; ++j) {
+        double lam = w[j];
+        if (j > i && lam - lam_prev < 10.0 * eps * scale) lam = lam_prev + 10.0 * eps * scale;
+        lam_prev = lam;
+        // LU with partial pivoting of T - lam I
+        for (int t = 0; t < n; ++t) {
+            D[t] = d[t] - lam;
+            if (t + 1 < n) {
+                DL[t] = ea[t];
+                DU[t] = ea[t];
+            }
+            DU2[t] = 0.0;
+            piv[t] = t;
+        }
+        for (int t = 0; t + 1 < n; ++t) {
+            if (fabs(D[t]) >= fabs(DL[t])) {
+                if (D[t] == 0.0) D[t] = tiny;
+                const double f = DL[t] / D[t];
+                DL[t] = f;
+                D[t + 1] -= f * DU[t];
+            } else {
+                const double f = D[t] / DL[t];
+                D[t] = DL[t];
+                DL[t] = f;
+                const double tmp = DU[t];
+                DU[t] = D[t + 1];
+                D[t + 1] = tmp - f * D[t + 1];
+                if (t + 2 < n) {
+                    DU2[t] = DU[t + 1];
+                    DU[t + 1] = -f * DU[t + 1];
+                }
+                piv[t] = t + 1;
+            }
+        }
+        for (int t = 0; t < n; ++t)
+            if (fabs(D[t]) < tiny) D[t] = D[t] < 0.0 ? -tiny : tiny;
+        double* y = Y + (size_t)j * n;
+        for (int t = 0; t < n; ++t) y[t] = 1.0 + 0.25 * sin(0.7 * t + 1.3 * j);
+        for (int iter = 0; iter < 3; ++iter) {
+            for (int t = 0; t + 1 < n; ++t) {
+                if (piv[t] == t) {
+                    y[t + 1] -= DL[t] * y[t];
+                } else {
+                    const double tmp = y[t];
+                    y[t] = y[t + 1];
+                    y[t + 1] = tmp - DL[t] * y[t];
+                }
+            }
+            y[n - 1] /= D[n - 1];
+            if (n > 1) y[n - 2] = (y[n - 2] - DU[n - 2] * y[n - 1]) / D[n - 2];
+            for (int t = n - 3; t >= 0; --t) y[t] = (y[t] - DU[t] * y[t + 1] - DU2[t] * y[t + 2]) / D[t];
+            for (int q = i; q < j; ++q) {
+                const double* yq = Y + (size_t)q * n;
+                double s = 0.0;
+                for (int t = 0; t < n; ++t) s += yq[t] * y[t];
+                for (int t = 0; t < n; ++t) y[t] -= s * yq[t];
+            }
+            double nr = 0.0;
+            for (int t = 0; t < n; ++t) nr += y[t] * y[t];
+            nr = 1.0 / sqrt(nr);
+            for (int t = 0; t < n; ++t) y[t] *= nr;
+        }
+    }
+}
+
+// Z[:, c] = Q (phase .* Y[:, c]), Q = H_0 H_1 ... H_{n-2}; one warp per column
+__global__ void herm_backtransform(int n, int nvec, const double2* Vh, const double* tau,
+                                   const double2* phase, const double* Y, double2* Z) {
+    const int lane = threadIdx.x & 31;
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c >= nvec) return;
+    double2* z = Z + (long)c * n;
+    const double* y = Y + (long)c * n;
+    for (int r = lane; r < n; r += 32) {
+        const double2 p = phase[r];
+        z[r] = mk(p.x * y[r], p.y * y[r]);
+    }
+    __syncwarp();
+    for (int k = n - 2; k >= 0; --k) {
+        const double t = tau[k];
+        if (t == 0.0) continue;
+        const int m = n - k - 1;
+        const double2* v = Vh + (long)k * n + (k + 1);
+        double2 s = mk(0.0, 0.0);
+        for (int j = lane; j < m; j += 32) s = s + cmulc(v[j], z[k + 1 + j]);
+        s = warp_sum(s);
+        s = mk(t * s.x, t * s.y);
+        for (int j = lane; j < m; j += 32) z[k + 1 + j] = z[k + 1 + j] - cmul(v[j], s);
+        __syncwarp();
+    }
+}
+
+struct Chol {
+    double2* dinv;
+    int* info;
+};
+
+Chol chol_take(Scratch& ws, int n) {
+    const int nblk = ceil_div(n, NB);
+    Chol c;
+    c.dinv = ws.take<double2>((size_t)nblk * NB * NB);
+    c.info = ws.take<int>(1);
+    return c;
+}
+
+int potrf_impl(cudaStream_t st, int n, double2* A, int lda, const Chol& c) {
+    const int nblk = ceil_div(n, NB);
+    Q3B_CUDA(cudaMemsetAsync(c.info, 0, sizeof(int), st));
+    for (int k = 0; k < nblk; ++k) {
+        potrf_diag<<<1, 256, 0, st>>>(n, k, A, lda, c.dinv, c.info);
+        Q3B_LAUNCH_CHECK();
+        const int m = nblk - k - 1;
+        if (m > 0) {
+            potrf_panel<<<m, 256, 0, st>>>(n, k, A, lda, c.dinv, c.info);
+            Q3B_LAUNCH_CHECK();
+            potrf_update<<<dim3(m, m), 256, 0, st>>>(n, k, A, lda, c.info);
+            Q3B_LAUNCH_CHECK();
+        }
+    }
+    int info = 0;
+    Q3B_CUDA(cudaMemcpyAsync(&info, c.info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    Q3B_CUDA(cudaStreamSynchronize(st));
+    return info;
+}
+
+void trtri_impl(cudaStream_t st, int n, const double2* A, int lda, const Chol& c, double2* Ui) {
+    const int nblk = ceil_div(n, NB);
+    Q3B_CUDA(cudaMemsetAsync(Ui, 0, (size_t)n * n * sizeof(double2), st));
+    trtri_diag<<<nblk, 256, 0, st>>>(n, c.dinv, Ui);
+    Q3B_LAUNCH_CHECK();
+    for (int j = 1; j < nblk; ++j) {
+        trtri_col<<<j, 256, 0, st>>>(n, j, A, lda, c.dinv, Ui);
+        Q3B_LAUNCH_CHECK();
+    }
+}
+
+}  // namespace
+
+size_t potrf_scratch_bytes(int n) {
+    const size_t nblk = (size_t)ceil_div(n, NB);
+    return nblk * NB * NB * sizeof(double2) + 1024;
+}
+
+size_t hegv_scratch_bytes(int n) {
+    // slices taken by hegv + heev: five n x n complex matrices (and the
+    // n x nvec eigenvector block), an n x n real block plus five more for
+    // inverse iteration, a few length-n vectors, and 256-byte alignment slack
+    const size_t nn = (size_t)n * n;
+    return potrf_scratch_bytes(n) + 6 * nn * sizeof(double2) + 6 * nn * sizeof(double) +
+           64 * (size_t)n * sizeof(double2) + 64 * 1024;
+}
+
+int potrf(cudaStream_t st, int n, double2* A, int lda, Scratch& ws) {
+    Chol c = chol_take(ws, n);
+    return potrf_impl(st, n, A, lda, c);
+}
+
+void trtri_after_potrf(cudaStream_t st, int n, const double2* A, int lda, double2* Uinv, Scratch& ws) {
+    Chol c = chol_take(ws, n);  // the slices potrf took first, still holding its block inverses
+    trtri_impl(st, n, A, lda, c, Uinv);
+}
+
+void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, Scratch& ws) {
+    if (n <= 0) return;
+    double* d = ws.take<double>(n);
+    double2* e = ws.take<double2>(n);
+    double* tau = ws.take<double>(n);
+    double2* Vh = ws.take<double2>((size_t)n * n);
+    double2* pbuf = ws.take<double2>(n);
+    double* ea = ws.take<double>(n);
+    double* e2 = ws.take<double>(n);
+    double2* phase = ws.take<double2>(n);
+    double* bounds = ws.take<double>(4);
+    double* Y = ws.take<double>((size_t)n * (nvec > 0 ? nvec : 1));
+    double* work = ws.take<double>((size_t)5 * n * (nvec > 0 ? nvec : 1));
+    int device = 0;
+    Q3B_CUDA(cudaGetDevice(&device));
+    int nsm = 0;
+    Q3B_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    int blocks = ceil_div(n, 8);
+    if (blocks > nsm) blocks = nsm;
+    if (blocks < 1) blocks = 1;
+    double2* partial = ws.take<double2>(blocks);
+    unsigned* bar = ws.take<unsigned>(2);
+    int* err = ws.take<int>(1);
+    Q3B_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
+    Q3B_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    Q3B_CUDA(cudaMemsetAsync(Vh, 0, (size_t)n * n * sizeof(double2), st));
+    const size_t smem = 2 * (size_t)n * sizeof(double2);
+    static bool attr_set = false;
+    if (!attr_set) {
+        Q3B_CUDA(cudaFuncSetAttribute(hetrd_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr_set = true;
+    }
+    int per_sm = 0;
+    Q3B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_coop, 256, smem));
+    if (per_sm < 1) throw Status(Q3B_ERR_INVALID, "subspace too large for the eigensolver");
+    void* args[] = {&n, &A, &d, &e, &Vh, &tau, &pbuf, &partial, &bar, &err};
+    Q3B_CUDA(cudaLaunchCooperativeKernel((const void*)hetrd_coop, dim3(blocks), dim3(256), args, smem, st));
+    Q3B_LAUNCH_CHECK();
+    tridiag_prep<<<1, 32, 0, st>>>(n, d, e, ea, e2, phase, bounds);
+    Q3B_LAUNCH_CHECK();
+    tridiag_multisect<<<ceil_div((long)n * 32, 256), 256, 0, st>>>(n, d, e2, bounds, w);
+    Q3B_LAUNCH_CHECK();
+    if (nvec > 0) {
+        tridiag_invit<<<ceil_div(nvec, 64), 64, 0, st>>>(n, d, ea, w, bounds, nvec, Y, work);
+        Q3B_LAUNCH_CHECK();
+        herm_backtransform<<<ceil_div((long)nvec * 32, 256), 256, 0, st>>>(n, nvec, Vh, tau, phase, Y, Z);
+        Q3B_LAUNCH_CHECK();
+    }
+    int herr = 0;
+    Q3B_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    Q3B_CUDA(cudaStreamSynchronize(st));
+    if (herr) throw Status(Q3B_ERR_INTERNAL, "eigensolver grid barrier timed out");
+}
+
+int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, double* w, double2* Z,
+         int nvec, Scratch& ws, const GemmWorkspace& gws) {
+    if (n <= 0) return 0;
+    const size_t nn = (size_t)n * n;
+    double2* Uw = ws.take<double2>(nn);
+    Chol c = chol_take(ws, n);
+    copy_matrix<<<grid_for((long)nn), 256, 0, st>>>(n, S, ld, Uw, n);
+    Q3B_LAUNCH_CHECK();
+    const int info = potrf_impl(st, n, Uw, n, c);
+    if (info != 0) return n + info;
+    double2* Ui = ws.take<double2>(nn);
+    trtri_impl(st, n, Uw, n, c, Ui);
+    double2* Hf = ws.take<double2>(nn);
+    hermitian_from_upper<<<grid_for((long)nn), 256, 0, st>>>(n, H, ld, Hf);
+    Q3B_LAUNCH_CHECK();
+    double2* W = ws.take<double2>(nn);
+    const double2 one = mk(1.0, 0.0), zero = mk(0.0, 0.0);
+    cgemm<double>(st, false, n, n, n, one, Hf, n, Ui, n, zero, W, n, gws);     // H U^{-1}
+    cgemm<double>(st, true, n, n, n, one, Ui, n, W, n, zero, Hf, n, gws);      // U^{-H} H U^{-1}
+    // make it exactly Hermitian from its upper triangle
+    hermitian_from_upper<<<grid_for((long)nn), 256, 0, st>>>(n, Hf, n, W);
+    Q3B_LAUNCH_CHECK();
+    double2* Zc = ws.take<double2>((size_t)n * (nvec > 0 ? nvec : 1));
+    heev(st, n, W, w, Zc, nvec, ws);
+    if (nvec > 0) cgemm<double>(st, false, n, nvec, n, one, Ui, n, Zc, n, zero, Z, n, gws);
+    return 0;
+}
+
+}  // namespace dense
+}  // namespace q3b

@@ -147,9 +147,39 @@ template <typename R> size_t plane_smem_bytes(const LocalPlan<R>& p) {
            (size_t)p.nrows * sizeof(int);
 }
 
+PhaseTimer::PhaseTimer() {
+    for (int i = 0; i < 2 * kMax; ++i) Q3B_CUDA(cudaEventCreate(&ev[i]));
+}
+PhaseTimer::~PhaseTimer() {
+    for (int i = 0; i < 2 * kMax; ++i) cudaEventDestroy(ev[i]);
+}
+void PhaseTimer::begin(int c) {
+    if (used >= kMax) return;
+    cls[used] = c;
+    Q3B_CUDA(cudaEventRecord(ev[2 * used], st));
+}
+void PhaseTimer::end() {
+    if (used >= kMax) return;
+    Q3B_CUDA(cudaEventRecord(ev[2 * used + 1], st));
+    ++used;
+}
+void PhaseTimer::collect(double* ms, int* count) {
+    Q3B_CUDA(cudaStreamSynchronize(st));
+    for (int c = 0; c < NCLASS; ++c) {
+        ms[c] = 0.0;
+        count[c] = 0;
+    }
+    for (int i = 0; i < used; ++i) {
+        float t = 0.f;
+        Q3B_CUDA(cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]));
+        ms[cls[i]] += t;
+        count[cls[i]] += 1;
+    }
+}
+
 template <typename R>
 void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, long ldpsi,
-                 cplx_t<R>* hpsi, long ldh, int nvec, cplx_t<R>* X, int chunk) {
+                 cplx_t<R>* hpsi, long ldh, int nvec, cplx_t<R>* X, int chunk, PhaseTimer* tm) {
     if (nvec <= 0) return;
     set_smem_limits<R>();
     if (chunk < 1) chunk = 1;
@@ -161,12 +191,18 @@ void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, l
         const cplx_t<R>* ps = psi + (long)b0 * ldpsi;
         cplx_t<R>* hs = hpsi + (long)b0 * ldh;
         if (p.nsticks > 0) {
+            if (tm) tm->begin(PhaseTimer::STICKS_BACKWARD);
             sticks_backward<R><<<dim3(nsg, nb), kStickThreads, smem_s, st>>>(p, ps, ldpsi, X);
             Q3B_LAUNCH_CHECK();
+            if (tm) tm->end();
+            if (tm) tm->begin(PhaseTimer::PLANES);
             planes<R><<<dim3(p.n3, nb), kPlaneThreads, smem_p, st>>>(p, X);
             Q3B_LAUNCH_CHECK();
+            if (tm) tm->end();
+            if (tm) tm->begin(PhaseTimer::STICKS_FORWARD);
             sticks_forward<R><<<dim3(nsg, nb), kStickThreads, smem_s, st>>>(p, X, ps, ldpsi, hs, ldh);
             Q3B_LAUNCH_CHECK();
+            if (tm) tm->end();
         }
     }
     if (p.nunmapped > 0) {
@@ -179,9 +215,9 @@ void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, l
 }
 
 template void apply_local<double>(cudaStream_t, const LocalPlan<double>&, const double2*, long,
-                                  double2*, long, int, double2*, int);
+                                  double2*, long, int, double2*, int, PhaseTimer*);
 template void apply_local<float>(cudaStream_t, const LocalPlan<float>&, const float2*, long,
-                                 float2*, long, int, float2*, int);
+                                 float2*, long, int, float2*, int, PhaseTimer*);
 template size_t plane_smem_bytes<double>(const LocalPlan<double>&);
 template size_t plane_smem_bytes<float>(const LocalPlan<float>&);
 

@@ -46,11 +46,28 @@ template <typename R> inline size_t sticks_bytes_per_band(const LocalPlan<R>& p)
     return (size_t)p.n3 * p.nsticks * sizeof(cplx_t<R>);
 }
 
+// Per-kernel-class CUDA-event timing of one application (diagnostics).
+struct PhaseTimer {
+    enum { STICKS_BACKWARD = 0, PLANES, STICKS_FORWARD, PROJ_OVERLAP, D_APPLY, PROJ_ACCUM, NCLASS };
+    static constexpr int kMax = 256;
+    cudaEvent_t ev[2 * kMax];
+    int cls[kMax];
+    int used = 0;
+    cudaStream_t st = nullptr;
+    PhaseTimer();
+    ~PhaseTimer();
+    void begin(int c);   // record the start of a launch of class c
+    void end();          // record its end
+    // synchronise and sum the durations per class (ms) and count launches
+    void collect(double* ms, int* count);
+};
+
 // hpsi[:, b] = KE*psi[:, b] + local term, for nvec bands (column stride ld).
 // X must hold chunk*sticks_bytes_per_band bytes.
 template <typename R>
 void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, long ldpsi,
-                 cplx_t<R>* hpsi, long ldh, int nvec, cplx_t<R>* X, int chunk);
+                 cplx_t<R>* hpsi, long ldh, int nvec, cplx_t<R>* X, int chunk,
+                 PhaseTimer* timer = nullptr);
 
 // shared-memory footprint of the plane kernel (for capacity checks)
 template <typename R> size_t plane_smem_bytes(const LocalPlan<R>& p);

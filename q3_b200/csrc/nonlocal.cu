@@ -54,15 +54,21 @@ inline int grid_for(long n) {
 template <typename R>
 void apply_nonlocal(cudaStream_t st, const NonlocalData<R>& nl, int npw, int nvec,
                     const cplx_t<R>* psi, long ldpsi, cplx_t<R>* hpsi, long ldh, cplx_t<R>* Bm,
-                    cplx_t<R>* Bp, const GemmWorkspace& ws) {
+                    cplx_t<R>* Bp, const GemmWorkspace& ws, PhaseTimer* tm) {
     using T = cplx_t<R>;
     if (nl.nproj <= 0 || nvec <= 0) return;
     const T one = mk(R(1), R(0)), zero = mk(R(0), R(0));
+    if (tm) tm->begin(PhaseTimer::PROJ_OVERLAP);
     cgemm<R>(st, true, nl.nproj, nvec, npw, one, nl.beta, npw, psi, ldpsi, zero, Bm, nl.nproj, ws);
+    if (tm) tm->end();
+    if (tm) tm->begin(PhaseTimer::D_APPLY);
     apply_d_blocks<R><<<grid_for((long)nl.nproj * nvec), 256, 0, st>>>(
         nl.nproj, nvec, nl.pstart, nl.psize, nl.poff, nl.dpk, Bm, Bp);
     Q3B_LAUNCH_CHECK();
+    if (tm) tm->end();
+    if (tm) tm->begin(PhaseTimer::PROJ_ACCUM);
     cgemm<R>(st, false, npw, nvec, nl.nproj, one, nl.beta, npw, Bp, nl.nproj, one, hpsi, ldh, ws);
+    if (tm) tm->end();
 }
 
 template <typename RI, typename RO>
@@ -74,10 +80,10 @@ void convert(cudaStream_t st, long n, const cplx_t<RI>* in, cplx_t<RO>* out) {
 
 template void apply_nonlocal<double>(cudaStream_t, const NonlocalData<double>&, int, int,
                                      const double2*, long, double2*, long, double2*, double2*,
-                                     const GemmWorkspace&);
+                                     const GemmWorkspace&, PhaseTimer*);
 template void apply_nonlocal<float>(cudaStream_t, const NonlocalData<float>&, int, int,
                                     const float2*, long, float2*, long, float2*, float2*,
-                                    const GemmWorkspace&);
+                                    const GemmWorkspace&, PhaseTimer*);
 template void convert<double, float>(cudaStream_t, long, const double2*, float2*);
 template void convert<float, double>(cudaStream_t, long, const float2*, double2*);
 template void convert<double, double>(cudaStream_t, long, const double2*, double2*);

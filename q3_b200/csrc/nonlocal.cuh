@@ -3,6 +3,7 @@
 
 #include "cgemm.cuh"
 #include "common.cuh"
+#include "hpsi_local.cuh"
 
 namespace q3b {
 
@@ -19,7 +20,7 @@ template <typename R> struct NonlocalData {
 template <typename R>
 void apply_nonlocal(cudaStream_t st, const NonlocalData<R>& nl, int npw, int nvec,
                     const cplx_t<R>* psi, long ldpsi, cplx_t<R>* hpsi, long ldh, cplx_t<R>* Bm,
-                    cplx_t<R>* Bp, const GemmWorkspace& ws);
+                    cplx_t<R>* Bp, const GemmWorkspace& ws, PhaseTimer* timer = nullptr);
 
 // out = (RO) in, n complex values
 template <typename RI, typename RO>

@@ -1,0 +1,170 @@
+"""Subspace eigensolver and Davidson on the GPU against the CPU oracle.
+
+Bars: the FP64 solve matches the oracle's FP64 Davidson within 1e-10 Ha
+(2e-10 Ry) on eigenvalues; the mixed solve (FP32 bulk + FP64 refinement)
+within 1e-8 Ha (2e-8 Ry) of the FP64 oracle.  The subspace eigensolver meets
+the reference's own known answers (test_subspace_diagonalizer.cpp).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import davidson as odav
+from oracle import hpsi as ohpsi
+from q3_b200 import synthetic
+from q3_b200._lib import FP64, MIXED, Q3BError
+
+pytestmark = pytest.mark.gpu
+
+FP64_EIG_TOL_RY = 2e-10     # 1e-10 Ha
+MIXED_EIG_TOL_RY = 2e-8     # 1e-8 Ha
+
+
+@pytest.fixture(scope="module")
+def ctx_app():
+    from q3_b200.applicator import PlanewaveHamiltonianApplicator
+    return PlanewaveHamiltonianApplicator()
+
+
+def _prep(ap, sy, k=0):
+    ap.update_potential(sy.v_r, sy.cell.grid)
+    ap.prepare_system_kpoint(sy, k)
+
+
+def test_hegv_kats(cuda_device, ctx_app):
+    from q3_b200.davidson import hegv
+    sy = synthetic.small_system()
+    _prep(ctx_app, sy)
+    w, z = hegv(ctx_app, np.array([[2, 0], [0, 3]], complex), np.eye(2))
+    assert np.allclose(w, [2, 3], atol=1e-10)
+    w, z = hegv(ctx_app, np.array([[2, 0], [0, 4]], complex), np.diag([1.0, 2.0]).astype(complex))
+    assert np.allclose(w, [2, 2], atol=1e-10)
+    w, z = hegv(ctx_app, np.array([[2, 1], [1, 2]], complex), np.eye(2))
+    assert np.allclose(w, [1, 3], atol=1e-10)
+
+
+def test_hegv_48_generalized(cuda_device, ctx_app):
+    from q3_b200.davidson import hegv
+    from tests.test_oracle import generalized_problem_48
+    h, s = generalized_problem_48()
+    w, z = hegv(ctx_app, h, s)
+    we = odav.diagonalize_subspace(h, s, 48)[0]
+    assert np.max(np.abs(w - we)) < 1e-11
+    assert np.max(np.abs(h @ z - (s @ z) * w[None, :])) < 1e-10
+    assert np.max(np.abs(z.conj().T @ s @ z - np.eye(48))) < 1e-10
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 31, 32, 33, 96, 200, 512])
+def test_hegv_random(cuda_device, ctx_app, n):
+    from q3_b200.davidson import hegv
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    h = (x + x.conj().T) / 2
+    q, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    s = np.eye(n) + 1e-3 * (q + q.conj().T) / 2
+    w, z = hegv(ctx_app, h, s)
+    we = odav.diagonalize_subspace(h, s, n)[0]
+    scale = max(1.0, np.max(np.abs(we)))
+    assert np.max(np.abs(w - we)) < 1e-12 * scale * max(1, n / 16)
+    assert np.max(np.abs(h @ z - (s @ z) * w[None, :])) < 1e-11 * scale * max(1, n / 16)
+
+
+def test_hegv_degenerate(cuda_device, ctx_app):
+    # exact degeneracies (as in symmetric cells): vectors stay S-orthonormal
+    from q3_b200.davidson import hegv
+    rng = np.random.default_rng(7)
+    n = 60
+    q, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    ev = np.round(rng.standard_normal(n) * 2.0)
+    h = q @ np.diag(ev) @ q.conj().T
+    w, z = hegv(ctx_app, h, np.eye(n))
+    assert np.max(np.abs(w - np.sort(ev))) < 1e-12
+    assert np.max(np.abs(z.conj().T @ z - np.eye(n))) < 1e-11
+
+
+def test_hegv_not_positive_definite(cuda_device, ctx_app):
+    from q3_b200.davidson import hegv
+    with pytest.raises(Q3BError):
+        hegv(ctx_app, np.eye(3, dtype=complex), np.diag([1.0, -1.0, 1.0]).astype(complex))
+
+
+def _oracle_solve(sy, k, tol, max_it, psi0=None):
+    kp = sy.kpoints[k]
+    return odav.solve(lambda x: ohpsi.apply_h(x, kp, sy.v_r, sy.cell.grid, threads=8), kp.ke,
+                      sy.psi0[k] if psi0 is None else psi0, sy.nbands, tol, max_iterations=max_it)
+
+
+def _gpu_solve(ap, sy, k, tol, max_it, precision=FP64, psi0=None, **kw):
+    from q3_b200.davidson import PlanewaveDavidsonDiagonalizer
+    _prep(ap, sy, k)
+    dv = PlanewaveDavidsonDiagonalizer(ap, precision)
+    dv.set_tolerance(tol)
+    dv.set_maximum_iterations(max_it)
+    for key, val in kw.items():
+        getattr(dv, key)(*val)
+    return dv.solve(sy.psi0[k] if psi0 is None else psi0, sy.nbands)
+
+
+def test_davidson_small_fp64(cuda_device, ctx_app):
+    sy = synthetic.small_system(nbands=6)
+    ref = _oracle_solve(sy, 0, 1e-10, 80)
+    got = _gpu_solve(ctx_app, sy, 0, 1e-10, 80)
+    assert got.unconverged == 0
+    assert np.max(np.abs(got.eigenvalues - ref.eigenvalues)) < FP64_EIG_TOL_RY
+
+
+def test_davidson_config0_golden(cuda_device, ctx_app):
+    g = np.load(Path(__file__).parent / "golden" / "config0_davidson.npz")
+    sy = synthetic.config(0)
+    got = _gpu_solve(ctx_app, sy, 0, 1e-10, 100)
+    assert got.unconverged == 0
+    assert np.max(np.abs(got.eigenvalues - g["eigenvalues"])) < FP64_EIG_TOL_RY
+    assert np.max(np.abs(got.eigenvalues - g["exact"])) < 1e-9
+    # the eigenvectors solve H psi = eps psi
+    kp = sy.kpoints[0]
+    r = ohpsi.apply_h(got.bands, kp, sy.v_r, sy.cell.grid) - got.bands * got.eigenvalues[None, :]
+    assert np.max(np.linalg.norm(r, axis=0)) < 1e-3
+
+
+def test_davidson_config0_mixed(cuda_device, ctx_app):
+    g = np.load(Path(__file__).parent / "golden" / "config0_davidson.npz")
+    sy = synthetic.config(0)
+    got = _gpu_solve(ctx_app, sy, 0, 1e-10, 100, precision=MIXED,
+                     set_precision=(MIXED, 1e-5, 8))
+    assert np.max(np.abs(got.eigenvalues - g["eigenvalues"])) < MIXED_EIG_TOL_RY
+    assert got.fp64_iterations < got.iterations
+
+
+def test_davidson_seeds_from_kinetic_energy(cuda_device, ctx_app):
+    # zero starting bands: the solve fills the basis from the lowest-KE plane waves
+    sy = synthetic.small_system(nbands=5)
+    kp = sy.kpoints[0]
+    zero = np.zeros((kp.npw, 5), complex)
+    ref = _oracle_solve(sy, 0, 1e-10, 80, psi0=zero)
+    got = _gpu_solve(ctx_app, sy, 0, 1e-10, 80, psi0=zero)
+    assert np.max(np.abs(got.eigenvalues - ref.eigenvalues)) < FP64_EIG_TOL_RY
+
+
+def test_davidson_config2_kpoint(cuda_device, ctx_app):
+    # an off-Gamma k-point of the 8-atom cell (npw ~ 3000, 48 bands, 40^3)
+    sy = synthetic.config(2, nk=2)
+    ref = _oracle_solve(sy, 1, 1e-9, 60)
+    got = _gpu_solve(ctx_app, sy, 1, 1e-9, 60)
+    assert np.max(np.abs(got.eigenvalues - ref.eigenvalues)) < 5 * FP64_EIG_TOL_RY
+    mixed = _gpu_solve(ctx_app, sy, 1, 1e-9, 60, precision=MIXED, set_precision=(MIXED, 1e-5, 10))
+    assert np.max(np.abs(mixed.eigenvalues - ref.eigenvalues)) < MIXED_EIG_TOL_RY
+
+
+def test_davidson_device_bands(cuda_device, ctx_app):
+    import torch
+    sy = synthetic.small_system(nbands=4)
+    _prep(ctx_app, sy)
+    from q3_b200.davidson import PlanewaveDavidsonDiagonalizer
+    dv = PlanewaveDavidsonDiagonalizer(ctx_app)
+    dv.set_tolerance(1e-10)
+    dv.set_maximum_iterations(80)
+    x = torch.from_numpy(np.ascontiguousarray(sy.psi0[0].T)).cuda()
+    res = dv.solve(x, 4)
+    host = _gpu_solve(ctx_app, sy, 0, 1e-10, 80)
+    assert np.max(np.abs(res.eigenvalues - host.eigenvalues)) < 1e-12
