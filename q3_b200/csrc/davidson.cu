@@ -278,13 +278,16 @@ template <typename R> class Davidson {
     }
 
     // --------------------------------------- diagonalize_subspace (serial.hpp:680-756)
-    // eigenvalues to w_ (and the first nb to host), eigenvectors (first nvec) to evec_ (ld n)
-    int diagonalize(int n, const double2* H, const double2* S, int ld) {
+    // eigenvalues to w_ (and, when `publish`, to the host copy the loop's
+    // convergence test reads), eigenvectors (first nvec) to evec_ (ld n).  The
+    // collapse diagonalises for its rotation only and does not publish, as the
+    // reference keeps those eigenvalues local (serial.hpp:838).
+    int diagonalize(int n, const double2* H, const double2* S, int ld, bool publish = true) {
         dscratch_.used = 0;
         const int nvec = std::min(nb_, n);
         GemmWorkspace gws = c_.gemm_ws(cgemm_workspace_bytes<double>(n, n, n));
         const int info = dense::hegv(st_, n, H, S, ld, w_, evec_, nvec, dscratch_, gws);
-        if (info == 0) {
+        if (info == 0 && publish) {
             whost_.assign(n, 0.0);
             Q3B_CUDA(cudaMemcpyAsync(whost_.data(), w_, n * sizeof(double), cudaMemcpyDeviceToHost, st_));
             Q3B_CUDA(cudaStreamSynchronize(st_));
@@ -321,7 +324,7 @@ template <typename R> class Davidson {
     // --------------------------------------- collapse_subspace (serial.hpp:825-945)
     int collapse(int basis, bool from_held) {
         int info = -1;
-        if (from_held) info = diagonalize(basis, Hs_, Ss_, maxn_);
+        if (from_held) info = diagonalize(basis, Hs_, Ss_, maxn_, false);
         if (info != 0) {
             // rebuild the subspace from the vectors
             T* h = coef_;
@@ -329,7 +332,7 @@ template <typename R> class Davidson {
             widen(basis, basis, h, basis, gram_, basis);
             gemm(true, basis, basis, npw_, one(), V_, npw_, V_, npw_, zero(), h, basis);
             widen(basis, basis, h, basis, uinv_, basis);
-            info = diagonalize(basis, gram_, uinv_, basis);
+            info = diagonalize(basis, gram_, uinv_, basis, false);
             if (info != 0) throw Status(Q3B_ERR_LINALG, "subspace eigensolver failed in the collapse");
         }
         rotate(basis);
