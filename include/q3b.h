@@ -104,6 +104,20 @@ int q3b_apply_h_f32(q3b_context* ctx, const q3b_cplx64* psi_dev, q3b_cplx64* hps
 int q3b_apply_h_host(q3b_context* ctx, const q3b_cplx128* psi_host, q3b_cplx128* hpsi_host,
                      int nvec, int precision);
 
+/* q3b_apply_h (FP64) for callers that cannot allocate device memory during the
+ * call: code inside a CUDA stream capture, runtimes that own all device memory
+ * through their own pool, or that forbid allocation once started.  No
+ * counterpart in the reference.  Its scratch (the stick buffer and the
+ * projector coefficients) is one fixed 32 MiB __device__ array that every GPU
+ * loading the library holds until exit; bands are processed in batches that
+ * fit it, and a k-point whose single band needs more is rejected with
+ * Q3B_ERR_INVALID.  The first call on a device looks the array up (with that
+ * device current) and should come before any stream capture.  Calls share the
+ * array, so calls that overlap on the GPU race.  Inputs and outputs are the
+ * caller's device buffers, as for q3b_apply_h. */
+int q3b_apply_h_noalloc(q3b_context* ctx, const q3b_cplx128* psi_dev, q3b_cplx128* hpsi_dev,
+                        int nvec);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 
 /* Per-kernel device time of one application, CUDA events around each launch

@@ -69,6 +69,7 @@ SIGNATURES = {
     "q3b_apply_h": (_i, [_vp, _vp, _vp, _i, _i]),
     "q3b_apply_h_f32": (_i, [_vp, _vp, _vp, _i]),
     "q3b_apply_h_host": (_i, [_vp, _vp, _vp, _i, _i]),
+    "q3b_apply_h_noalloc": (_i, [_vp, _vp, _vp, _i]),
     "q3b_apply_h_timed": (_i, [_vp, _vp, _vp, _i, _i, C.POINTER(ApplyTiming)]),
     "q3b_kernel_launches": (C.c_ulonglong, []),
     "q3b_davidson_default_opts": (None, [C.POINTER(DavidsonOpts)]),
