@@ -150,7 +150,10 @@ typedef struct {
     int occupied_bands;          /* bands held to `tolerance`; the rest to max(5 tol, 1e-5)  */
     int precision;               /* Q3B_FP64 or Q3B_MIXED                                   */
     int refine_sweeps;           /* MIXED: max FP64 refinement iterations at the end         */
-    double mixed_tolerance;      /* MIXED: eigenvalue-change tolerance of the FP32 phase, Ry */
+    double mixed_tolerance;      /* MIXED: eigenvalue-change tolerance of the FP32 phase, Ry;
+                                    the phase also ends once the change stops falling       */
+    int profile_stages;          /* nonzero: fill q3b_davidson_stats.stage_ms (drains the
+                                    stream at every stage boundary)                         */
 } q3b_davidson_opts;
 
 typedef struct {
@@ -161,6 +164,10 @@ typedef struct {
     int collapses;
     double max_residual_norm;    /* max_i ||H psi_i - eps_i psi_i|| of the returned bands   */
     double seconds;              /* wall time of the solve                                   */
+    double stage_ms[8];          /* with profile_stages: seed, diagonalize, correction,
+                                    orthogonalize, hamiltonian, subspace_update, collapse,
+                                    extract (the reference's DavidsonTimingAccumulator
+                                    stages, counters.hpp:36-52)                             */
 } q3b_davidson_stats;
 
 void q3b_davidson_default_opts(q3b_davidson_opts* opts);

@@ -42,13 +42,17 @@ class DavidsonOpts(C.Structure):
     _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_int),
                 ("basis_expansion_factor", C.c_int), ("occupied_bands", C.c_int),
                 ("precision", C.c_int), ("refine_sweeps", C.c_int),
-                ("mixed_tolerance", C.c_double)]
+                ("mixed_tolerance", C.c_double), ("profile_stages", C.c_int)]
 
 
 class DavidsonStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("fp64_iterations", C.c_int),
                 ("h_applications", C.c_int), ("unconverged", C.c_int), ("collapses", C.c_int),
-                ("max_residual_norm", C.c_double), ("seconds", C.c_double)]
+                ("max_residual_norm", C.c_double), ("seconds", C.c_double),
+                ("stage_ms", C.c_double * 8)]
+
+    STAGES = ("seed", "diagonalize", "correction", "orthogonalize", "hamiltonian",
+              "subspace_update", "collapse", "extract")
 
 
 _vp, _i, _d, _sz = C.c_void_p, C.c_int, C.c_double, C.c_size_t

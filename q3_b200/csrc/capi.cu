@@ -176,8 +176,9 @@ void q3b_davidson_default_opts(q3b_davidson_opts* o) {
     o->basis_expansion_factor = 2; // davidson.hpp:864
     o->occupied_bands = 0;         // 0: every band is occupied
     o->precision = Q3B_FP64;
-    o->refine_sweeps = 6;
-    o->mixed_tolerance = 1e-5;
+    o->refine_sweeps = 8;
+    o->mixed_tolerance = 1e-6;
+    o->profile_stages = 0;
 }
 
 int q3b_davidson_solve_dev(q3b_context* ctx, q3b_cplx128* bands, double* eig, int nb,

@@ -144,6 +144,34 @@ __global__ void column_norms(int npw, const cplx_t<R>* __restrict__ X, double* o
     if (threadIdx.x == 0) out[blockIdx.x] = sqrt(red[0]);
 }
 
+__global__ void set_identity(int n, double2* E) {
+    const long total = (long)n * n;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x)
+        E[t] = (t % n == t / n) ? mk(1.0, 0.0) : mk(0.0, 0.0);
+}
+
+// Host-side stage clock in the spirit of the reference's stage_time_point
+// (davidson.hpp:942-956): the stream is drained before each reading, so a
+// stage is charged for the device work it queued.
+struct StageClock {
+    cudaStream_t st = nullptr;
+    double* ms = nullptr;  // 8 stages, or null when not profiling
+    std::chrono::steady_clock::time_point t;
+    void start() {
+        if (!ms) return;
+        Q3B_CUDA(cudaStreamSynchronize(st));
+        t = std::chrono::steady_clock::now();
+    }
+    void stop(int stage) {
+        if (!ms) return;
+        Q3B_CUDA(cudaStreamSynchronize(st));
+        const auto now = std::chrono::steady_clock::now();
+        ms[stage] += std::chrono::duration<double, std::milli>(now - t).count();
+        t = now;
+    }
+};
+enum Stage { SEED = 0, DIAG, CORR, ORTHO, HAPPLY, UPDATE, COLLAPSE, EXTRACT };
+
 // carve one device buffer into slices
 struct Carve {
     char* base;
@@ -340,6 +368,13 @@ template <typename R> class Davidson {
         Q3B_CUDA(cudaMemsetAsync(Hs_, 0, mm * sizeof(double2), st_));
         Q3B_CUDA(cudaMemsetAsync(Ss_, 0, mm * sizeof(double2), st_));
         update(0, nb_, nb_);
+        // The next iteration's subspace is the nb Ritz vectors just formed: its
+        // matrices are diag(w) and the identity to rounding, so its eigenpairs
+        // are these eigenvalues (left in w_[0, nb)) and unit vectors.
+        collapse_w_.assign(nb_, 0.0);
+        Q3B_CUDA(cudaMemcpyAsync(collapse_w_.data(), w_, nb_ * sizeof(double), cudaMemcpyDeviceToHost, st_));
+        Q3B_CUDA(cudaStreamSynchronize(st_));
+        reuse_collapse_ = true;
         return nb_;
     }
 
@@ -387,11 +422,19 @@ template <typename R> class Davidson {
         std::vector<double> eig;
         int iterations = 0, unconverged = 0, collapses = 0;
         double resid = 0.0;
+        bool stagnated = false;
     };
 
+    // stagnate: stop (with the Ritz pairs of this iteration) once the largest
+    // eigenvalue change has stopped halving for three iterations while below
+    // 1e-3 Ry -- the FP32 phase of the mixed solve has then reached what its
+    // precision can resolve.
     Result solve(int seeded, const std::vector<double>& stored, double tol, int max_it, int occupied,
-                 T* out, bool want_resid) {
+                 T* out, bool want_resid, double* stage_ms = nullptr, bool stagnate = false) {
         Result res;
+        StageClock clk{st_, stage_ms};
+        reuse_collapse_ = false;
+        clk.start();
         int basis = orthogonalize(0, seeded);                            // :1000-1045
         apply(0, basis);
         if (basis < nb_) {                                                // :1047-1101
@@ -414,7 +457,9 @@ template <typename R> class Davidson {
             throw Status(Q3B_ERR_LINALG, "could not build " + std::to_string(nb_) +
                                              " independent starting vectors");
         update(0, basis, basis);                                          // :459-469
+        clk.stop(SEED);
         std::vector<double> prev(nb_, 0.0);
+        std::vector<double> history;
         bool have_stored = false;
         for (double e : stored) have_stored = have_stored || e != 0.0;
         if (have_stored) {
@@ -425,7 +470,15 @@ template <typename R> class Davidson {
         }
         const double empty_tol = std::max(kEmptyRelax * tol, kEmptyFloor);
         for (int it = 0; it < max_it; ++it) {                            // :498
-            int info = diagonalize(basis, Hs_, Ss_, maxn_);
+            int info = 0;
+            if (reuse_collapse_ && basis == nb_) {
+                whost_ = collapse_w_;
+                set_identity<<<grid_for((long)nb_ * nb_), 256, 0, st_>>>(nb_, evec_);
+                Q3B_LAUNCH_CHECK();
+            } else {
+                info = diagonalize(basis, Hs_, Ss_, maxn_);
+            }
+            reuse_collapse_ = false;
             if (info != 0 && basis > nb_) {                               // :521-590
                 basis = collapse(basis, false);
                 ++res.collapses;
@@ -437,34 +490,58 @@ template <typename R> class Davidson {
             } else if (info != 0) {
                 throw Status(Q3B_ERR_LINALG, "subspace eigensolver failed");
             }
+            clk.stop(DIAG);
             ++res.iterations;
             std::vector<int> unconv;
+            double maxchange = 0.0;
             for (int b = 0; b < nb_; ++b) {                               // :615-629
                 const double change = std::fabs(whost_[b] - prev[b]);
+                maxchange = std::max(maxchange, change);
                 const double tb = b < occupied ? tol : empty_tol;
                 if (!(it != 0 && change < tb)) unconv.push_back(b);
             }
             res.unconverged = static_cast<int>(unconv.size());
-            if (unconv.empty()) {                                         // :649-668
+            if (it != 0) history.push_back(maxchange);
+            const size_t h = history.size();
+            const bool stalled = stagnate && h >= 4 && history[h - 1] < 1e-3 &&
+                                 history[h - 1] > 0.5 * history[h - 4];
+            if (unconv.empty() || stalled) {                              // :649-668
+                res.stagnated = stalled && !unconv.empty();
                 extract(basis, out, want_resid ? &res.resid : nullptr);
+                clk.stop(EXTRACT);
                 res.eig.assign(whost_.begin(), whost_.begin() + nb_);
                 return res;
             }
             const int ncand = corrections(basis, unconv, maxn_ - basis);  // :689-703
+            clk.stop(CORR);
             const int acc = orthogonalize(basis, ncand);                  // :705-712
+            clk.stop(ORTHO);
             apply(basis, acc);                                            // :728-738
+            clk.stop(HAPPLY);
             const int old = basis;
             basis += acc;
             if (acc > 0) update(old, acc, basis);                         // :743-760
+            clk.stop(UPDATE);
             if (basis >= maxn_) {                                         // :763-808
                 basis = collapse(basis, true);
                 ++res.collapses;
             }
+            clk.stop(COLLAPSE);
             for (int b = 0; b < nb_; ++b) prev[b] = whost_[b];
         }
-        const int info = diagonalize(basis, Hs_, Ss_, maxn_);             // :816-840
+        int info = 0;                                                     // :816-840
+        if (reuse_collapse_ && basis == nb_) {
+            whost_ = collapse_w_;
+            set_identity<<<grid_for((long)nb_ * nb_), 256, 0, st_>>>(nb_, evec_);
+            Q3B_LAUNCH_CHECK();
+        } else {
+            info = diagonalize(basis, Hs_, Ss_, maxn_);
+        }
+        reuse_collapse_ = false;
         if (info != 0) throw Status(Q3B_ERR_LINALG, "subspace eigensolver failed at exit");
+        clk.stop(DIAG);
         extract(basis, out, want_resid ? &res.resid : nullptr);
+        clk.stop(EXTRACT);
         res.eig.assign(whost_.begin(), whost_.begin() + nb_);
         return res;
     }
@@ -501,6 +578,8 @@ template <typename R> class Davidson {
     const double* ke_;
     dense::Scratch dscratch_;
     std::vector<double> whost_;
+    std::vector<double> collapse_w_;
+    bool reuse_collapse_ = false;
 };
 
 }  // namespace
@@ -520,7 +599,8 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
     if (o.precision == Q3B_FP64) {
         Davidson<double> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
         Q3B_CUDA(cudaMemcpyAsync(dv.V(), bands_dev, band_bytes, cudaMemcpyDeviceToDevice, c.stream));
-        auto r = dv.solve(nb, stored, o.tolerance, std::max(1, o.max_iterations), occupied, bands_dev, true);
+        auto r = dv.solve(nb, stored, o.tolerance, std::max(1, o.max_iterations), occupied, bands_dev, true,
+                          o.profile_stages ? s.stage_ms : nullptr);
         std::copy(r.eig.begin(), r.eig.end(), eig_host);
         s.iterations = s.fp64_iterations = r.iterations;
         s.h_applications = dv.happly();
@@ -534,9 +614,9 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         {
             Davidson<float> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
             convert<double, float>(c.stream, (long)npw * nb, bands_dev, dv.V());
-            const double tol32 = o.mixed_tolerance > 0.0 ? o.mixed_tolerance : 1e-5;
+            const double tol32 = o.mixed_tolerance > 0.0 ? o.mixed_tolerance : 1e-6;
             auto r = dv.solve(nb, stored, std::max(tol32, o.tolerance), std::max(1, o.max_iterations),
-                              occupied, dv.scratch(), false);
+                              occupied, dv.scratch(), false, o.profile_stages ? s.stage_ms : nullptr, true);
             // widen the FP32 Ritz vectors into the caller's bands
             convert<float, double>(c.stream, (long)npw * nb, dv.scratch(), bands_dev);
             eig32 = r.eig;
@@ -548,7 +628,8 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         Davidson<double> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
         Q3B_CUDA(cudaMemcpyAsync(dv.V(), bands_dev, band_bytes, cudaMemcpyDeviceToDevice, c.stream));
         const int sweeps = o.refine_sweeps > 0 ? o.refine_sweeps : 6;
-        auto r = dv.solve(nb, eig32, o.tolerance, sweeps, occupied, bands_dev, true);
+        auto r = dv.solve(nb, eig32, o.tolerance, sweeps, occupied, bands_dev, true,
+                          o.profile_stages ? s.stage_ms : nullptr);
         std::copy(r.eig.begin(), r.eig.end(), eig_host);
         s.iterations = it32 + r.iterations;
         s.fp64_iterations = r.iterations;

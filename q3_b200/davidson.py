@@ -29,6 +29,7 @@ class SolveResult:
     collapses: int
     max_residual_norm: float
     seconds: float
+    stage_ms: dict
 
 
 class PlanewaveDavidsonDiagonalizer:
@@ -60,6 +61,9 @@ class PlanewaveDavidsonDiagonalizer:
     def set_occupied_bands(self, n: int) -> None:
         self.opts.occupied_bands = int(n)
 
+    def set_profile_stages(self, on: bool = True) -> None:
+        self.opts.profile_stages = 1 if on else 0
+
     def solve(self, bands, number_of_bands: int,
               stored_eigenvalues: Optional[np.ndarray] = None) -> SolveResult:
         """bands: npw x nb numpy array (host) or a torch complex128 CUDA tensor
@@ -79,8 +83,9 @@ class PlanewaveDavidsonDiagonalizer:
                                                  C.byref(self.opts), C.byref(st))
             out = bands
         check(h, rc)
+        stages = dict(zip(DavidsonStats.STAGES, list(st.stage_ms)))
         return SolveResult(eig, out, st.iterations, st.fp64_iterations, st.h_applications,
-                           st.unconverged, st.collapses, st.max_residual_norm, st.seconds)
+                           st.unconverged, st.collapses, st.max_residual_norm, st.seconds, stages)
 
 
 def hegv(applicator, h: np.ndarray, s: np.ndarray):
