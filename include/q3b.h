@@ -118,6 +118,21 @@ int q3b_apply_h_host(q3b_context* ctx, const q3b_cplx128* psi_host, q3b_cplx128*
 int q3b_apply_h_noalloc(q3b_context* ctx, const q3b_cplx128* psi_dev, q3b_cplx128* hpsi_dev,
                         int nvec);
 
+/* ---- complex GEMMs of the subspace algebra --------------------------------- */
+
+/* The reference's GPU BLAS products (GPUBLAS::gemm / gemm_single,
+ * src/layer_0_core/math/linear_algebra/gpu/blas/init.hpp:70-82,136-148) as the
+ * path uses them: C = alpha op(A) B + beta C, column-major, device pointers,
+ * transpose_a 'N' or 'C', transpose_b 'N'.  q3b_gemm runs in FP64 on the CUDA
+ * cores; q3b_gemm_single runs on the tensor cores (TF32 split into hi + lo,
+ * three products, FP32 accumulation: FP32 accuracy).  Queued on the stream. */
+int q3b_gemm(q3b_context* ctx, char transpose_a, char transpose_b, int m, int n, int k,
+             q3b_cplx128 alpha, const q3b_cplx128* a_dev, int lda, const q3b_cplx128* b_dev, int ldb,
+             q3b_cplx128 beta, q3b_cplx128* c_dev, int ldc);
+int q3b_gemm_single(q3b_context* ctx, char transpose_a, char transpose_b, int m, int n, int k,
+                    q3b_cplx64 alpha, const q3b_cplx64* a_dev, int lda, const q3b_cplx64* b_dev, int ldb,
+                    q3b_cplx64 beta, q3b_cplx64* c_dev, int ldc);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 
 /* Per-kernel device time of one application, CUDA events around each launch

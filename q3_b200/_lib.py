@@ -25,6 +25,14 @@ class Q3BError(RuntimeError):
         self.code = code
 
 
+class Cplx128(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
+class Cplx64(C.Structure):
+    _fields_ = [("re", C.c_float), ("im", C.c_float)]
+
+
 class ApplyTiming(C.Structure):
     _fields_ = [("sticks_backward_ms", C.c_double), ("planes_ms", C.c_double),
                 ("sticks_forward_ms", C.c_double), ("projector_overlap_ms", C.c_double),
@@ -76,6 +84,9 @@ SIGNATURES = {
     "q3b_apply_h_noalloc": (_i, [_vp, _vp, _vp, _i]),
     "q3b_apply_h_timed": (_i, [_vp, _vp, _vp, _i, _i, C.POINTER(ApplyTiming)]),
     "q3b_kernel_launches": (C.c_ulonglong, []),
+    "q3b_gemm": (_i, [_vp, C.c_char, C.c_char, _i, _i, _i, Cplx128, _vp, _i, _vp, _i, Cplx128, _vp, _i]),
+    "q3b_gemm_single": (_i, [_vp, C.c_char, C.c_char, _i, _i, _i, Cplx64, _vp, _i, _vp, _i, Cplx64, _vp,
+                             _i]),
     "q3b_davidson_default_opts": (None, [C.POINTER(DavidsonOpts)]),
     "q3b_davidson_solve": (_i, [_vp, _vp, _vp, _i, C.POINTER(DavidsonOpts), C.POINTER(DavidsonStats)]),
     "q3b_davidson_solve_dev": (_i, [_vp, _vp, _vp, _i, C.POINTER(DavidsonOpts),

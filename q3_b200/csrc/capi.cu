@@ -20,6 +20,23 @@ template <typename F> int guarded(q3b_context* c, F&& f) {
     }
 }
 
+template <typename R, typename CT>
+void gemm_entry(Context& c, char ta, char tb, int m, int n, int k, CT alpha, const CT* a, int lda,
+                       const CT* b, int ldb, CT beta, CT* cc, int ldc) {
+    using T = q3b::cplx_t<R>;
+    const bool conj = (ta == 'C' || ta == 'c');
+    if (!(conj || ta == 'N' || ta == 'n') || !(tb == 'N' || tb == 'n'))
+        throw q3b::Status(Q3B_ERR_INVALID, "gemm: transpose_a must be N or C and transpose_b N");
+    if (m < 0 || n < 0 || k < 0) throw q3b::Status(Q3B_ERR_INVALID, "gemm: negative size");
+    if (m == 0 || n == 0) return;
+    if ((k > 0 && (!a || !b)) || !cc) throw q3b::Status(Q3B_ERR_INVALID, "gemm: null matrix");
+    if (lda < (conj ? k : m) || ldb < k || ldc < m || lda < 1 || ldb < 1)
+        throw q3b::Status(Q3B_ERR_INVALID, "gemm: leading dimension too small");
+    q3b::GemmWorkspace ws = c.gemm_ws(conj ? q3b::cgemm_workspace_bytes<R>(m, n, k) : 0);
+    q3b::cgemm<R>(c.stream, conj, m, n, k, T{alpha.re, alpha.im}, reinterpret_cast<const T*>(a), lda,
+                  reinterpret_cast<const T*>(b), ldb, T{beta.re, beta.im}, reinterpret_cast<T*>(cc), ldc, ws);
+}
+
 }  // namespace
 
 extern "C" {
@@ -59,7 +76,10 @@ int q3b_set_stream(q3b_context* ctx, void* s) {
 }
 
 int q3b_synchronize(q3b_context* ctx) {
-    return guarded(ctx, [&](Context& c) { Q3B_CUDA(cudaStreamSynchronize(c.stream)); });
+    return guarded(ctx, [&](Context& c) {
+        Q3B_CUDA(cudaStreamSynchronize(c.stream));
+        q3b::tc::check_error(c.stream);
+    });
 }
 
 size_t q3b_device_bytes(const q3b_context* ctx) { return ctx ? ctx->impl.held : 0; }
@@ -130,6 +150,7 @@ int q3b_apply_h_host(q3b_context* ctx, const q3b_cplx128* psi, q3b_cplx128* hpsi
         if (rc != Q3B_OK) throw q3b::Status(rc, c.err);
         Q3B_CUDA(cudaMemcpyAsync(hpsi, dout, n * sizeof(double2), cudaMemcpyDeviceToHost, c.stream));
         Q3B_CUDA(cudaStreamSynchronize(c.stream));
+        q3b::tc::check_error(c.stream);
     });
 }
 
@@ -147,6 +168,7 @@ int q3b_apply_h_timed(q3b_context* ctx, const void* psi, void* hpsi, int nvec, i
         double ms[q3b::PhaseTimer::NCLASS];
         int cnt[q3b::PhaseTimer::NCLASS];
         tm.collect(ms, cnt);
+        q3b::tc::check_error(c.stream);
         if (timing) {
             timing->sticks_backward_ms = ms[0];
             timing->planes_ms = ms[1];
@@ -160,6 +182,16 @@ int q3b_apply_h_timed(q3b_context* ctx, const void* psi, void* hpsi, int nvec, i
 }
 
 unsigned long long q3b_kernel_launches(void) { return q3b::launches(); }
+
+int q3b_gemm(q3b_context* ctx, char ta, char tb, int m, int n, int k, q3b_cplx128 alpha, const q3b_cplx128* a,
+             int lda, const q3b_cplx128* b, int ldb, q3b_cplx128 beta, q3b_cplx128* cc, int ldc) {
+    return guarded(ctx, [&](Context& c) { gemm_entry<double>(c, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, cc, ldc); });
+}
+
+int q3b_gemm_single(q3b_context* ctx, char ta, char tb, int m, int n, int k, q3b_cplx64 alpha, const q3b_cplx64* a,
+                    int lda, const q3b_cplx64* b, int ldb, q3b_cplx64 beta, q3b_cplx64* cc, int ldc) {
+    return guarded(ctx, [&](Context& c) { gemm_entry<float>(c, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, cc, ldc); });
+}
 
 }  // extern "C"
 
@@ -176,7 +208,7 @@ void q3b_davidson_default_opts(q3b_davidson_opts* o) {
     o->basis_expansion_factor = 2; // davidson.hpp:864
     o->occupied_bands = 0;         // 0: every band is occupied
     o->precision = Q3B_FP64;
-    o->refine_sweeps = 8;
+    o->refine_sweeps = 30;
     o->mixed_tolerance = 1e-6;
     o->profile_stages = 0;
 }

@@ -1,4 +1,6 @@
 // Complex GEMMs on CUDA cores; see cgemm.cuh.
+#include <type_traits>
+
 #include "cgemm.cuh"
 
 namespace q3b {
@@ -169,6 +171,7 @@ template <typename R> int choose_splits(int M, int N, int K) {
 }  // namespace
 
 template <typename R> size_t cgemm_workspace_bytes(int M, int N, int K) {
+    if constexpr (std::is_same<R, float>::value) return tc::workspace_bytes(M, N, K);
     const int s = choose_splits<R>(M, N, K);
     return s > 1 ? (size_t)s * M * N * sizeof(cplx_t<R>) : 0;
 }
@@ -180,6 +183,12 @@ void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, cplx_t<R> alpha, c
     using T = cplx_t<R>;
     if (M <= 0 || N <= 0) return;
     constexpr int BK = GemmTile<R>::BK;
+    if constexpr (std::is_same<R, float>::value) {
+        if (K > 0) {
+            tc::cgemm(st, conj_a, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, ws);
+            return;
+        }
+    }
     if (K <= 0) {
         // C = beta * C
         dim3 g(ceil_div((long)M * N, 256));

@@ -28,4 +28,15 @@ void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, cplx_t<R> alpha, c
 // bytes of workspace cgemm may use for a C,N product of this shape
 template <typename R> size_t cgemm_workspace_bytes(int M, int N, int K);
 
+// The FP32 products run on the tensor cores (cgemm_tc.cu).
+namespace tc {
+void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, const float2* A, long lda,
+           const float2* B, long ldb, float2 beta, float2* C, long ldc, const GemmWorkspace& ws);
+size_t workspace_bytes(int M, int N, int K);
+// device word the tensor-core kernels set when a pipeline wait times out
+int* error_word();
+// read (and clear) it; throws CudaError when it was set.  Synchronises st.
+void check_error(cudaStream_t st);
+}  // namespace tc
+
 }  // namespace q3b

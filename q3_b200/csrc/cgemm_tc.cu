@@ -1,0 +1,478 @@
+// Complex FP32 GEMMs on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+//   "C,N":  C = alpha A^H B + beta C    (A: K x M, lda; B: K x N, ldb)
+//   "N,N":  C = alpha A B   + beta C    (A: M x K, lda; B: K x N, ldb)
+//
+// Complex products are split into real products on planes (re, im) of each
+// operand, and every real operand x is split into two TF32 numbers,
+// x = hi + lo with hi = rn_tf32(x), lo = rn_tf32(x - hi); a real product is
+// then hi*hi + hi*lo + lo*hi accumulated in FP32 in TMEM (the lo*lo term,
+// ~2^-22 relative, is dropped).  That keeps FP32 accuracy at tensor-core rate.
+//
+// Block tile: 128 (M) x 64 (N) complex outputs, K in blocks of 32.  Warps 0-3
+// load a K block of A and B with coalesced 16-byte loads, split and
+// de-interleave it into eight operand planes (A re/im hi/lo, B re/im hi/lo),
+// each row 32 TF32 values = one 128-byte swizzle row (K-major, SWIZZLE_128B),
+// and signal a "full" mbarrier.  One thread of warp 4 issues the 48
+// tcgen05.mma (4 K-steps x 12 real products) of the block into two FP32
+// accumulators in TMEM (Re: columns 0-63, Im: 64-127) and commits to the
+// stage's "empty" mbarrier.  Two stages.  After the last block warps 0-3 read
+// the accumulators back with tcgen05.ld (one TMEM lane per output row) and
+// write C, or the raw sums of their K range for a fixed-order split-K
+// reduction.  Every mbarrier wait is bounded; a timeout sets an error word
+// and the block drains and frees its TMEM.
+#include <cstdint>
+
+#include "cgemm.cuh"
+
+namespace q3b {
+namespace tc {
+namespace {
+
+constexpr int BM = 128;            // complex rows per block (UMMA M)
+constexpr int BN = 64;             // complex columns per block (UMMA N)
+constexpr int BK = 32;             // K per stage: one 128-byte TF32 row
+constexpr int STAGES = 2;
+constexpr int PRODUCERS = 128;     // warps 0-3
+constexpr int THREADS = PRODUCERS + 32;
+constexpr int A_PLANE = BM * 128;  // bytes of one A plane (BM rows x 128 B)
+constexpr int B_PLANE = BN * 128;
+constexpr int STAGE_BYTES = 4 * A_PLANE + 4 * B_PLANE;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
+// Re in columns [0, 64), Im in [64, 128); 256 are allocated (one block per
+// SM, so TMEM is not shared) to keep the accumulators well inside the allocation.
+constexpr uint32_t TMEM_COLS = 256;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait on an mbarrier phase; false (and the error word set) on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+    for (int i = 0; i < (1 << 22); ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (*reinterpret_cast<volatile int*>(err)) return false;
+        if (i > 32) __nanosleep(64);
+    }
+    atomicExch(err, 1);
+    return false;
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor: K-major, SWIZZLE_128B, rows of 128 B,
+// 8-row groups 1024 B apart (SBO), version 1 (sm_100).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((addr >> 4) & 0x3FFF);
+    d |= static_cast<uint64_t>(1) << 16;                 // LBO (unused for swizzled K-major)
+    d |= static_cast<uint64_t>((1024 >> 4) & 0x3FFF) << 32;
+    d |= static_cast<uint64_t>(1) << 46;                 // version
+    d |= static_cast<uint64_t>(2) << 61;                 // SWIZZLE_128B
+    return d;
+}
+
+// Instruction descriptor: kind::tf32, D f32, A/B tf32 K-major, M = 128, N = 64.
+__host__ __device__ constexpr uint32_t instr_desc(bool negate_a) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((negate_a ? 1u : 0u) << 13) |
+           (static_cast<uint32_t>(BN >> 3) << 17) | (static_cast<uint32_t>(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float tf32_rn(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// byte offset of (row, k) in a 128B-swizzled K-major plane of TF32
+__device__ __forceinline__ uint32_t swz(int row, int k) {
+    return static_cast<uint32_t>(row * 128 + ((((k >> 2) ^ (row & 7))) << 4) + ((k & 3) << 2));
+}
+
+// Split two complex values (re0, im0, re1, im1) at K positions k, k+1 of one
+// operand row into the four planes (re hi, re lo, im hi, im lo).
+__device__ __forceinline__ void put_pair(unsigned char* planes, int plane_bytes, int row, int k, float4 v,
+                                         bool conj) {
+    const float re0 = v.x, re1 = v.z;
+    const float im0 = conj ? -v.y : v.y, im1 = conj ? -v.w : v.w;
+    const float rh0 = tf32_rn(re0), rh1 = tf32_rn(re1), ih0 = tf32_rn(im0), ih1 = tf32_rn(im1);
+    const float rl0 = tf32_rn(re0 - rh0), rl1 = tf32_rn(re1 - rh1);
+    const float il0 = tf32_rn(im0 - ih0), il1 = tf32_rn(im1 - ih1);
+    const uint32_t o = swz(row, k);
+    *reinterpret_cast<float2*>(planes + 0 * plane_bytes + o) = make_float2(rh0, rh1);
+    *reinterpret_cast<float2*>(planes + 1 * plane_bytes + o) = make_float2(rl0, rl1);
+    *reinterpret_cast<float2*>(planes + 2 * plane_bytes + o) = make_float2(ih0, ih1);
+    *reinterpret_cast<float2*>(planes + 3 * plane_bytes + o) = make_float2(il0, il1);
+}
+
+// Four K values (k..k+3) of one operand row, as a 16-byte chunk per plane.
+__device__ __forceinline__ void put_quad(unsigned char* planes, int plane_bytes, int row, int k, const float2* c) {
+    float rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        rh[j] = tf32_rn(c[j].x);
+        rl[j] = tf32_rn(c[j].x - rh[j]);
+        ih[j] = tf32_rn(c[j].y);
+        il[j] = tf32_rn(c[j].y - ih[j]);
+    }
+    const uint32_t o = swz(row, k);
+    *reinterpret_cast<float4*>(planes + 0 * plane_bytes + o) = make_float4(rh[0], rh[1], rh[2], rh[3]);
+    *reinterpret_cast<float4*>(planes + 1 * plane_bytes + o) = make_float4(rl[0], rl[1], rl[2], rl[3]);
+    *reinterpret_cast<float4*>(planes + 2 * plane_bytes + o) = make_float4(ih[0], ih[1], ih[2], ih[3]);
+    *reinterpret_cast<float4*>(planes + 3 * plane_bytes + o) = make_float4(il[0], il[1], il[2], il[3]);
+}
+
+// One K block of a K-contiguous operand (column `row` of X holds K values):
+// rows [r0, r0+nrows) of the tile, K in [k0, k0+32).  Each half-warp reads one
+// row's 256 bytes; conj negates the imaginary part.
+__device__ __forceinline__ void load_kmajor(unsigned char* planes, int plane_bytes, int nrows, const float2* X,
+                                            long ldx, int r0, int rmax, int k0, int kend, bool conj, int tid) {
+    for (int idx = tid; idx < nrows * 16; idx += PRODUCERS) {
+        const int row = idx >> 4;
+        const int kp = (idx & 15) * 2;  // even K offset within the block
+        const int gr = r0 + row, gk = k0 + kp;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (gr < rmax) {
+            const float2* p = X + (long)gr * ldx + gk;
+            if (gk + 1 < kend && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
+                v = *reinterpret_cast<const float4*>(p);
+            } else {
+                if (gk < kend) { const float2 a = p[0]; v.x = a.x; v.y = a.y; }
+                if (gk + 1 < kend) { const float2 b = p[1]; v.z = b.x; v.w = b.y; }
+            }
+        }
+        put_pair(planes, plane_bytes, row, kp, v, conj);
+    }
+}
+
+// One K block of an M-contiguous operand (A of "N,N": element (m, k) at
+// X[m + k*ldx]): each thread takes two rows and four K values.
+__device__ __forceinline__ void load_mmajor(unsigned char* planes, int plane_bytes, const float2* X, long ldx,
+                                            int m0, int mmax, int k0, int kend, int tid) {
+    for (int idx = tid; idx < (BM / 2) * (BK / 4); idx += PRODUCERS) {
+        const int mp = idx % (BM / 2);
+        const int kq = idx / (BM / 2);
+        const int row = 2 * mp, gm = m0 + row;
+        float2 c0[4], c1[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int gk = k0 + kq * 4 + j;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (gk < kend && gm < mmax) {
+                const float2* p = X + (long)gk * ldx + gm;
+                if (gm + 1 < mmax && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
+                    v = *reinterpret_cast<const float4*>(p);
+                } else {
+                    const float2 a = p[0];
+                    v.x = a.x;
+                    v.y = a.y;
+                    if (gm + 1 < mmax) { const float2 b = p[1]; v.z = b.x; v.w = b.y; }
+                }
+            }
+            c0[j] = make_float2(v.x, v.y);
+            c1[j] = make_float2(v.z, v.w);
+        }
+        put_quad(planes, plane_bytes, row, kq * 4, c0);
+        put_quad(planes, plane_bytes, row + 1, kq * 4, c1);
+    }
+}
+
+template <bool CONJ_A>
+__global__ void __launch_bounds__(THREADS, 1)
+cgemm_tc_kernel(int M, int N, int K, float2 alpha, const float2* __restrict__ A, long lda,
+                const float2* __restrict__ B, long ldb, float2 beta, float2* C, long ldc, int kchunk,
+                float2* part, int* err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[STAGES];
+    __shared__ __align__(8) uint64_t empty_bar[STAGES];
+    __shared__ __align__(8) uint64_t done_bar;
+    __shared__ uint32_t tmem_slot;
+
+    unsigned char* smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int kbeg = blockIdx.z * kchunk;
+    const int kend = min(K, kbeg + kchunk);
+    const int nkb = kend > kbeg ? (kend - kbeg + BK - 1) / BK : 0;
+
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full_bar[s], PRODUCERS);
+            mbar_init(&empty_bar[s], 1);
+        }
+        mbar_init(&done_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp < 4) {
+        // ---------------------------------------------------------- producers
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % STAGES;
+            if (kb >= STAGES && !mbar_wait(&empty_bar[s], ((kb / STAGES) - 1) & 1, err)) break;
+            unsigned char* st = smem + s * STAGE_BYTES;
+            unsigned char* pa = st;
+            unsigned char* pb = st + 4 * A_PLANE;
+            const int k0 = kbeg + kb * BK;
+            if (CONJ_A)
+                load_kmajor(pa, A_PLANE, BM, A, lda, m0, M, k0, kend, false, tid);
+            else
+                load_mmajor(pa, A_PLANE, A, lda, m0, M, k0, kend, tid);
+            load_kmajor(pb, B_PLANE, BN, B, ldb, n0, N, k0, kend, false, tid);
+            fence_async_smem();
+            mbar_arrive(&full_bar[s]);
+        }
+    } else if (lane == 0) {
+        // ------------------------------------------------------- MMA issuer
+        // real products: (A plane, B plane, accumulator, negate A)
+        // C,N: Re += ar br + ai bi      Im += ar bi - ai br
+        // N,N: Re += ar br - ai bi      Im += ar bi + ai br
+        bool first_re = true, first_im = true;
+        bool ok = true;
+        for (int kb = 0; kb < nkb && ok; ++kb) {
+            const int s = kb % STAGES;
+            if (!mbar_wait(&full_bar[s], (kb / STAGES) & 1, err)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
+            const uint32_t a_base = base, b_base = base + 4 * A_PLANE;
+#pragma unroll
+            for (int ks = 0; ks < BK / 8; ++ks) {
+                const uint32_t off = ks * 32;
+#pragma unroll
+                for (int t = 0; t < 12; ++t) {
+                    const int prod = t / 3;           // 0: r*r 1: i*i 2: r*i 3: i*r
+                    const int term = t % 3;           // 0: hi*hi 1: hi*lo 2: lo*hi
+                    const int ap = (prod == 0 || prod == 2) ? 0 : 2;
+                    const int bp = (prod == 0 || prod == 3) ? 0 : 2;
+                    const int a_plane = ap + (term == 2 ? 1 : 0);
+                    const int b_plane = bp + (term == 1 ? 1 : 0);
+                    const bool to_im = prod >= 2;
+                    bool neg;
+                    if (CONJ_A) neg = (prod == 3);
+                    else neg = (prod == 1);
+                    const uint64_t ad = smem_desc(a_base + a_plane * A_PLANE + off);
+                    const uint64_t bd = smem_desc(b_base + b_plane * B_PLANE + off);
+                    const uint32_t d = tmem + (to_im ? BN : 0);
+                    bool& first = to_im ? first_im : first_re;
+                    mma_tf32(d, ad, bd, instr_desc(neg), first ? 0u : 1u);
+                    first = false;
+                }
+            }
+            mma_commit(&empty_bar[s]);
+        }
+        mma_commit(&done_bar);
+    }
+
+    // ------------------------------------------------------------ epilogue
+    if (warp < 4) {
+        const bool waited = nkb > 0 && mbar_wait(&done_bar, 0, err);
+        const bool have = __all_sync(0xffffffffu, waited);  // tcgen05.ld is warp-collective
+        tc_fence_after();
+        const int row = m0 + warp * 32 + lane;
+        const uint32_t lane_addr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+        const bool use_beta = (beta.x != 0.f || beta.y != 0.f);
+#pragma unroll
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            float re[16], im[16];
+            if (have) {
+                tmem_ld16(lane_addr + c0, re);
+                tmem_ld16(lane_addr + BN + c0, im);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) re[j] = im[j] = 0.f;
+            }
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int col = n0 + c0 + j;
+                    if (col >= N) break;
+                    const float2 acc = make_float2(re[j], im[j]);
+                    if (part) {
+                        part[(long)blockIdx.z * M * N + (long)col * M + row] = acc;
+                    } else {
+                        float2 v = make_float2(alpha.x * acc.x - alpha.y * acc.y, alpha.x * acc.y + alpha.y * acc.x);
+                        float2* cp = C + row + (long)col * ldc;
+                        if (use_beta) {
+                            const float2 o = *cp;
+                            v.x += beta.x * o.x - beta.y * o.y;
+                            v.y += beta.x * o.y + beta.y * o.x;
+                        }
+                        *cp = v;
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS)
+                     : "memory");
+    }
+}
+
+__global__ void splitk_sum(int M, int N, int splits, const float2* __restrict__ part, float2 alpha, float2 beta,
+                           float2* C, long ldc) {
+    const long total = (long)M * N;
+    const bool use_beta = (beta.x != 0.f || beta.y != 0.f);
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+        const int m = static_cast<int>(idx % M), n = static_cast<int>(idx / M);
+        float2 s = part[idx];
+        for (int z = 1; z < splits; ++z) {
+            const float2 p = part[(long)z * total + idx];
+            s.x += p.x;
+            s.y += p.y;
+        }
+        float2 v = make_float2(alpha.x * s.x - alpha.y * s.y, alpha.x * s.y + alpha.y * s.x);
+        float2* cp = C + m + (long)n * ldc;
+        if (use_beta) {
+            const float2 o = *cp;
+            v.x += beta.x * o.x - beta.y * o.y;
+            v.y += beta.x * o.y + beta.y * o.x;
+        }
+        *cp = v;
+    }
+}
+
+int choose_splits(int M, int N, int K) {
+    const int tiles = ceil_div(M, BM) * ceil_div(N, BN);
+    int s = ceil_div(148, tiles);
+    const int kmax = ceil_div(K, 256);
+    if (s > kmax) s = kmax;
+    if (s < 1) s = 1;
+    if (s > 64) s = 64;
+    return s;
+}
+
+__device__ int g_tc_error;
+
+}  // namespace
+
+int* error_word() {
+    static int* addr[64] = {};
+    int dev = 0;
+    Q3B_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
+    if (!addr[dev]) {
+        void* p = nullptr;
+        Q3B_CUDA(cudaGetSymbolAddress(&p, g_tc_error));
+        addr[dev] = static_cast<int*>(p);
+    }
+    return addr[dev];
+}
+
+void check_error(cudaStream_t st) {
+    int* w = error_word();
+    int h = 0;
+    Q3B_CUDA(cudaMemcpyAsync(&h, w, sizeof(int), cudaMemcpyDeviceToHost, st));
+    Q3B_CUDA(cudaStreamSynchronize(st));
+    if (h) {
+        Q3B_CUDA(cudaMemsetAsync(w, 0, sizeof(int), st));
+        throw CudaError("tensor-core GEMM: a pipeline wait timed out");
+    }
+}
+
+size_t workspace_bytes(int M, int N, int K) {
+    const int s = choose_splits(M, N, K);
+    return s > 1 ? (size_t)s * M * N * sizeof(float2) : 0;
+}
+
+void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, const float2* A, long lda,
+           const float2* B, long ldb, float2 beta, float2* C, long ldc, const GemmWorkspace& ws) {
+    int* err = error_word();
+    static bool attr = false;
+    if (!attr) {
+        Q3B_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+        Q3B_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+        attr = true;
+    }
+    int splits = conj_a ? choose_splits(M, N, K) : 1;
+    const size_t need = (size_t)splits * M * N * sizeof(float2);
+    if (splits > 1 && (ws.ptr == nullptr || ws.bytes < need)) splits = 1;
+    int kchunk = K;
+    if (splits > 1) {
+        kchunk = ceil_div(ceil_div(K, splits), BK) * BK;
+        splits = ceil_div(K, kchunk);
+    }
+    dim3 grid(ceil_div(M, BM), ceil_div(N, BN), splits);
+    float2* part = splits > 1 ? static_cast<float2*>(ws.ptr) : nullptr;
+    if (conj_a)
+        cgemm_tc_kernel<true><<<grid, THREADS, SMEM_BYTES, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                                 kchunk, part, err);
+    else
+        cgemm_tc_kernel<false><<<grid, THREADS, SMEM_BYTES, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                                  kchunk, part, err);
+    Q3B_LAUNCH_CHECK();
+    if (splits > 1) {
+        const long total = (long)M * N;
+        int blocks = ceil_div(total, 256);
+        if (blocks > 4096) blocks = 4096;
+        splitk_sum<<<blocks, 256, 0, st>>>(M, N, splits, part, alpha, beta, C, ldc);
+        Q3B_LAUNCH_CHECK();
+    }
+}
+
+}  // namespace tc
+}  // namespace q3b

@@ -52,6 +52,7 @@ struct KPoint {
     DevBuf tw64[3], tw32[3];
     LocalPlan<double> lp64{};
     LocalPlan<float> lp32{};
+    bool tuned64 = false, tuned32 = false;
 };
 
 class Context {
@@ -72,7 +73,7 @@ class Context {
 
     // workspaces
     DevBuf ws_sticks, ws_gemm, ws_bm, ws_bp, ws_conv_in, ws_conv_out, ws_host_io;
-    DevBuf ws_solver, ws_dense, ws_bands;
+    DevBuf ws_solver, ws_dense, ws_bands, ws_tune;
 
     explicit Context(int dev, size_t hbm_budget);
     ~Context();
@@ -92,6 +93,10 @@ class Context {
                  PhaseTimer* timer = nullptr);
 
     GemmWorkspace gemm_ws(size_t need);
+
+    // Autotuner: time the candidate plane kernels on a few bands of this
+    // k-point and keep the fastest (once per plan and precision).
+    template <typename R> void tune_local();
 
   private:
     void build_plan();

@@ -34,6 +34,7 @@ constexpr double kNormThreshold = 1e-14;    // tolerances.hpp:39
 constexpr double kPrecondFloor = 1e-4;      // tolerances.hpp:50
 constexpr double kEmptyRelax = 5.0;         // tolerances.hpp:65
 constexpr double kEmptyFloor = 1e-5;        // tolerances.hpp:66
+constexpr double kStallBelow = 1e-5;        // Ry: the FP32 phase may stop on a plateau below this
 
 inline int grid_for(long n) {
     long b = (n + 255) / 256;
@@ -427,8 +428,8 @@ template <typename R> class Davidson {
 
     // stagnate: stop (with the Ritz pairs of this iteration) once the largest
     // eigenvalue change has stopped halving for three iterations while below
-    // 1e-3 Ry -- the FP32 phase of the mixed solve has then reached what its
-    // precision can resolve.
+    // kStallBelow -- near the FP32 resolution of the eigenvalues, where the FP32
+    // phase of the mixed solve can go no further.
     Result solve(int seeded, const std::vector<double>& stored, double tol, int max_it, int occupied,
                  T* out, bool want_resid, double* stage_ms = nullptr, bool stagnate = false) {
         Result res;
@@ -503,7 +504,7 @@ template <typename R> class Davidson {
             res.unconverged = static_cast<int>(unconv.size());
             if (it != 0) history.push_back(maxchange);
             const size_t h = history.size();
-            const bool stalled = stagnate && h >= 4 && history[h - 1] < 1e-3 &&
+            const bool stalled = stagnate && h >= 4 && history[h - 1] < kStallBelow &&
                                  history[h - 1] > 0.5 * history[h - 4];
             if (unconv.empty() || stalled) {                              // :649-668
                 res.stagnated = stalled && !unconv.empty();
@@ -641,6 +642,7 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         throw Status(Q3B_ERR_INVALID, "unknown precision");
     }
     Q3B_CUDA(cudaStreamSynchronize(c.stream));
+    tc::check_error(c.stream);
     s.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (stats) *stats = s;
 }

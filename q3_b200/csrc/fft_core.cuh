@@ -151,14 +151,15 @@ struct NoEpilogue {
     template <typename T> __device__ __forceinline__ T operator()(int, int, T v) const { return v; }
 };
 
-// step 1: in place, no hazard between items
+// step 1: in place, no hazard between items.  Item it = l + lines*n2; the
+// (l, n2) pair is stepped by blockDim without dividing in the loop.
 template <int NA, int DIR, typename T>
 __device__ __forceinline__ void line_step1(T* buf, const LineGeom& g, const T* tw) {
     const int items = g.lines * g.nb;
     const int tws = g.n / NA;
+    const int bq = static_cast<int>(blockDim.x) / g.lines, br = static_cast<int>(blockDim.x) % g.lines;
+    int l = static_cast<int>(threadIdx.x) % g.lines, n2 = static_cast<int>(threadIdx.x) / g.lines;
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int l = it % g.lines;
-        const int n2 = it / g.lines;
         T* p = buf + g.base(l) + n2 * g.es;
         T x[NA];
 #pragma unroll
@@ -169,6 +170,12 @@ __device__ __forceinline__ void line_step1(T* buf, const LineGeom& g, const T* t
             const int m = n2 * k1;  // < n
             T v = (k1 == 0 || n2 == 0) ? x[k1] : cmul(x[k1], twiddle<DIR>(tw, m));
             p[k1 * g.nb * g.es] = v;
+        }
+        l += br;
+        n2 += bq;
+        if (l >= g.lines) {
+            l -= g.lines;
+            ++n2;
         }
     }
 }
@@ -185,14 +192,29 @@ __device__ __forceinline__ void line_step2(T* buf, const LineGeom& g, const T* t
     for (int l0 = 0; l0 < g.lines; l0 += per_round) {
         const int lr = min(per_round, g.lines - l0);
         const int items = lr * g.na;
+        const int bq = static_cast<int>(blockDim.x) / lr, br = static_cast<int>(blockDim.x) % lr;
+        const int lt = static_cast<int>(threadIdx.x) % lr, kt = static_cast<int>(threadIdx.x) / lr;
         T x[MAXIT][NB];
+        int ls[MAXIT], ks[MAXIT];
+        {
+            int l = lt, k1 = kt;
+#pragma unroll
+            for (int r = 0; r < MAXIT; ++r) {
+                ls[r] = l0 + l;
+                ks[r] = k1;
+                l += br;
+                k1 += bq;
+                if (l >= lr) {
+                    l -= lr;
+                    ++k1;
+                }
+            }
+        }
 #pragma unroll
         for (int r = 0; r < MAXIT; ++r) {
             const int it = threadIdx.x + r * blockDim.x;
             if (it < items) {
-                const int l = l0 + it % lr;
-                const int k1 = it / lr;
-                const T* p = buf + g.base(l) + k1 * g.nb * g.es;
+                const T* p = buf + g.base(ls[r]) + ks[r] * g.nb * g.es;
 #pragma unroll
                 for (int n2 = 0; n2 < NB; ++n2) x[r][n2] = p[n2 * g.es];
             }
@@ -202,8 +224,8 @@ __device__ __forceinline__ void line_step2(T* buf, const LineGeom& g, const T* t
         for (int r = 0; r < MAXIT; ++r) {
             const int it = threadIdx.x + r * blockDim.x;
             if (it < items) {
-                const int l = l0 + it % lr;
-                const int k1 = it / lr;
+                const int l = ls[r];
+                const int k1 = ks[r];
                 dft<NB, DIR>(x[r], tw, tws);
                 T* p = buf + g.base(l);
 #pragma unroll

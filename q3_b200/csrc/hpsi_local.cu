@@ -6,6 +6,7 @@
 // forward 3D FFT, hpsi += grid[map].  The 3D transforms are factored into
 // stick (w3) and plane (w1, w2) transforms that never touch empty sticks.
 #include <mutex>
+#include <type_traits>
 
 #include "fft_core.cuh"
 #include "hpsi_local.cuh"
@@ -46,7 +47,7 @@ sticks_backward(LocalPlan<R> p, const cplx_t<R>* __restrict__ psi, long ldpsi, c
     }
     __syncthreads();
     fft::LineGeom g{p.n3, p.na3, p.nb3, ns, p.p3, 1, nullptr};
-    fft::lines<+1, 1>(lines, g, tw, fft::NoEpilogue{});
+    fft::lines<+1, 2>(lines, g, tw, fft::NoEpilogue{});
     T* xb = X + (long)band * p.n3 * p.nsticks;
     for (int idx = threadIdx.x; idx < ns * p.n3; idx += blockDim.x) {
         const int s = idx % ns, i3 = idx / ns;
@@ -54,8 +55,10 @@ sticks_backward(LocalPlan<R> p, const cplx_t<R>* __restrict__ psi, long ldpsi, c
     }
 }
 
-// pass B: one (band, w3) plane per block
-template <typename R>
+// pass B: one (band, w3) plane per block.  MI = items of the second line step
+// a thread holds at once: more per thread means fewer barrier rounds but more
+// registers (fewer resident blocks); the autotuner picks it per plan.
+template <typename R, int MI>
 __global__ void __launch_bounds__(kPlaneThreads) planes(LocalPlan<R> p, cplx_t<R>* X) {
     using T = cplx_t<R>;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -74,10 +77,10 @@ __global__ void __launch_bounds__(kPlaneThreads) planes(LocalPlan<R> p, cplx_t<R
     __syncthreads();
     fft::LineGeom gr{p.n2, p.na2, p.nb2, p.nrows, 0, 1, rowb};
     fft::LineGeom gc{p.n1, p.na1, p.nb1, p.n2, 1, p.p2, nullptr};
-    fft::lines<+1, 1>(plane, gr, tw2, fft::NoEpilogue{});
-    fft::lines<+1, 1>(plane, gc, tw1, VEpilogue<R>{p.vplane + (long)i3 * p.n1 * p.n2, p.n2});
-    fft::lines<-1, 1>(plane, gc, tw1, fft::NoEpilogue{});
-    fft::lines<-1, 1>(plane, gr, tw2, fft::NoEpilogue{});
+    fft::lines<+1, MI>(plane, gr, tw2, fft::NoEpilogue{});
+    fft::lines<+1, MI>(plane, gc, tw1, VEpilogue<R>{p.vplane + (long)i3 * p.n1 * p.n2, p.n2});
+    fft::lines<-1, MI>(plane, gc, tw1, fft::NoEpilogue{});
+    fft::lines<-1, MI>(plane, gr, tw2, fft::NoEpilogue{});
     for (int s = threadIdx.x; s < p.nsticks; s += blockDim.x) xp[s] = plane[p.stick_pos[s]];
 }
 
@@ -101,7 +104,7 @@ sticks_forward(LocalPlan<R> p, const cplx_t<R>* __restrict__ X, const cplx_t<R>*
     }
     __syncthreads();
     fft::LineGeom g{p.n3, p.na3, p.nb3, ns, p.p3, 1, nullptr};
-    fft::lines<-1, 1>(lines, g, tw, fft::NoEpilogue{});
+    fft::lines<-1, 2>(lines, g, tw, fft::NoEpilogue{});
     const T* ps = psi + (long)band * ldpsi;
     T* hs = hpsi + (long)band * ldh;
     const int e0 = p.stick_start[s0], e1 = p.stick_start[s0 + ns];
@@ -134,7 +137,9 @@ template <typename R> void set_smem_limits() {
     static std::once_flag once;
     std::call_once(once, [] {
         const int lim = 227 * 1024;
-        cudaFuncSetAttribute(planes<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(planes<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(planes<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(planes<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
         cudaFuncSetAttribute(sticks_backward<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
         cudaFuncSetAttribute(sticks_forward<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     });
@@ -196,7 +201,13 @@ void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, l
             Q3B_LAUNCH_CHECK();
             if (tm) tm->end();
             if (tm) tm->begin(PhaseTimer::PLANES);
-            planes<R><<<dim3(p.n3, nb), kPlaneThreads, smem_p, st>>>(p, X);
+            const dim3 gp(p.n3, nb);
+            if (p.plane_items >= 4 && !std::is_same<R, double>::value)
+                planes<R, 4><<<gp, kPlaneThreads, smem_p, st>>>(p, X);
+            else if (p.plane_items >= 2)
+                planes<R, 2><<<gp, kPlaneThreads, smem_p, st>>>(p, X);
+            else
+                planes<R, 1><<<gp, kPlaneThreads, smem_p, st>>>(p, X);
             Q3B_LAUNCH_CHECK();
             if (tm) tm->end();
             if (tm) tm->begin(PhaseTimer::STICKS_FORWARD);

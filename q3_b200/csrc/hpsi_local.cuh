@@ -26,6 +26,7 @@ template <typename R> struct LocalPlan {
     int p3;             // pitch of a stick line in shared memory (odd)
     int na1, nb1, na2, nb2, na3, nb3;
     int sg;             // sticks per block in passes A and C
+    int plane_items;    // second-step items per thread in the plane kernel (1, 2, 4)
     int nunmapped;      // G outside the grid: kinetic term only
     const int* stick_start;  // nsticks+1, ranges into the entry arrays
     const int* entry_g;      // G index (caller's order) of each sphere entry

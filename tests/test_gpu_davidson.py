@@ -152,7 +152,7 @@ def test_davidson_config2_kpoint(cuda_device, ctx_app):
     ref = _oracle_solve(sy, 1, 1e-9, 60)
     got = _gpu_solve(ctx_app, sy, 1, 1e-9, 60)
     assert np.max(np.abs(got.eigenvalues - ref.eigenvalues)) < 5 * FP64_EIG_TOL_RY
-    mixed = _gpu_solve(ctx_app, sy, 1, 1e-9, 60, precision=MIXED, set_precision=(MIXED, 1e-5, 10))
+    mixed = _gpu_solve(ctx_app, sy, 1, 1e-9, 60, precision=MIXED, set_precision=(MIXED, 1e-6, 40))
     assert np.max(np.abs(mixed.eigenvalues - ref.eigenvalues)) < MIXED_EIG_TOL_RY
 
 
