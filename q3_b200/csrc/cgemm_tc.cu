@@ -3,24 +3,27 @@
 //   "C,N":  C = alpha A^H B + beta C    (A: K x M, lda; B: K x N, ldb)
 //   "N,N":  C = alpha A B   + beta C    (A: M x K, lda; B: K x N, ldb)
 //
-// Complex products are split into real products on planes (re, im) of each
-// operand, and every real operand x is split into two TF32 numbers,
-// x = hi + lo with hi = rn_tf32(x), lo = rn_tf32(x - hi); a real product is
-// then hi*hi + hi*lo + lo*hi accumulated in FP32 in TMEM (the lo*lo term,
-// ~2^-22 relative, is dropped).  That keeps FP32 accuracy at tensor-core rate.
+// Every real operand x is split into two TF32 numbers, x = hi + lo with
+// hi = rn_tf32(x), lo = rn_tf32(x - hi); a real product is hi*hi + hi*lo +
+// lo*hi accumulated in FP32 in TMEM (the lo*lo term, ~2^-22 relative, is
+// dropped), which keeps FP32 accuracy at tensor-core rate.
 //
-// Block tile: 128 (M) x 64 (N) complex outputs, K in blocks of 32.  Warps 0-3
-// load a K block of A and B with coalesced 16-byte loads, split and
-// de-interleave it into eight operand planes (A re/im hi/lo, B re/im hi/lo),
-// each row 32 TF32 values = one 128-byte swizzle row (K-major, SWIZZLE_128B),
-// and signal a "full" mbarrier.  One thread of warp 4 issues the 48
-// tcgen05.mma (4 K-steps x 12 real products) of the block into two FP32
-// accumulators in TMEM (Re: columns 0-63, Im: 64-127) and commits to the
-// stage's "empty" mbarrier.  Two stages.  After the last block warps 0-3 read
-// the accumulators back with tcgen05.ld (one TMEM lane per output row) and
-// write C, or the raw sums of their K range for a fixed-order split-K
-// reduction.  Every mbarrier wait is bounded; a timeout sets an error word
-// and the block drains and frees its TMEM.
+// Block tile: 128 (M) x 64 (N) complex outputs, K in blocks of 32.  The A
+// operand is held as four planes (re hi, re lo, im hi, im lo), 128 rows each;
+// the B operand as two planes (hi, lo) of 128 rows: rows 0-63 the real parts
+// of the 64 columns, rows 64-127 their imaginary parts.  Each row is 32 TF32
+// values = one 128-byte swizzle row (K-major, SWIZZLE_128B).  Per K step of 8
+// one thread issues six tcgen05.mma of 128 x 128 x 8:
+//   P = Ar [Br | Bi]^T  and  Q = Ai [Br | Bi]^T   (x3 for the split terms)
+// into two FP32 accumulators of 128 TMEM columns, and the epilogue forms
+//   C,N: Re = P_r + Q_i,  Im = P_i - Q_r      N,N: Re = P_r - Q_i,  Im = P_i + Q_r.
+// Warps 0-3 load a K block with coalesced 16-byte loads (all issued before any
+// conversion), split and de-interleave it into the planes and signal a "full"
+// mbarrier; the MMA thread commits each stage to an "empty" mbarrier; two
+// stages.  After the last block warps 0-3 read the accumulators with
+// tcgen05.ld (one TMEM lane per output row) and write C, or the raw sums of
+// their K range for a fixed-order split-K reduction.  Every mbarrier wait is
+// bounded; a timeout sets an error word and the block drains and frees TMEM.
 #include <cstdint>
 
 #include "cgemm.cuh"
@@ -35,12 +38,12 @@ constexpr int BK = 32;             // K per stage: one 128-byte TF32 row
 constexpr int STAGES = 2;
 constexpr int PRODUCERS = 128;     // warps 0-3
 constexpr int THREADS = PRODUCERS + 32;
-constexpr int A_PLANE = BM * 128;  // bytes of one A plane (BM rows x 128 B)
-constexpr int B_PLANE = BN * 128;
-constexpr int STAGE_BYTES = 4 * A_PLANE + 4 * B_PLANE;
+constexpr int A_PLANE = BM * 128;      // bytes of one A plane (BM rows x 128 B)
+constexpr int B_PLANE = 2 * BN * 128;  // bytes of one B plane (re rows + im rows)
+constexpr int UMMA_N = 2 * BN;         // [Br | Bi]
+constexpr int STAGE_BYTES = 4 * A_PLANE + 2 * B_PLANE;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
-// Re in columns [0, 64), Im in [64, 128); 256 are allocated (one block per
-// SM, so TMEM is not shared) to keep the accumulators well inside the allocation.
+// P in columns [0, 128), Q in [128, 256) (one block per SM: TMEM is not shared)
 constexpr uint32_t TMEM_COLS = 256;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -91,10 +94,10 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
     return d;
 }
 
-// Instruction descriptor: kind::tf32, D f32, A/B tf32 K-major, M = 128, N = 64.
-__host__ __device__ constexpr uint32_t instr_desc(bool negate_a) {
-    return (1u << 4) | (2u << 7) | (2u << 10) | ((negate_a ? 1u : 0u) << 13) |
-           (static_cast<uint32_t>(BN >> 3) << 17) | (static_cast<uint32_t>(BM >> 4) << 24);
+// Instruction descriptor: kind::tf32, D f32, A/B tf32 K-major, M = 128, N = 128.
+__host__ __device__ constexpr uint32_t instr_desc() {
+    return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(UMMA_N >> 3) << 17) |
+           (static_cast<uint32_t>(BM >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -170,57 +173,123 @@ __device__ __forceinline__ void put_quad(unsigned char* planes, int plane_bytes,
 }
 
 // One K block of a K-contiguous operand (column `row` of X holds K values):
-// rows [r0, r0+nrows) of the tile, K in [k0, k0+32).  Each half-warp reads one
-// row's 256 bytes; conj negates the imaginary part.
-__device__ __forceinline__ void load_kmajor(unsigned char* planes, int plane_bytes, int nrows, const float2* X,
-                                            long ldx, int r0, int rmax, int k0, int kend, bool conj, int tid) {
-    for (int idx = tid; idx < nrows * 16; idx += PRODUCERS) {
+// rows [r0, r0+NROWS) of the tile, K in [k0, k0+32).  Each half-warp reads one
+// row's 256 bytes.  All of a thread's loads are issued before any is
+// converted, so a K block costs one memory latency, not one per load.
+template <int NROWS>
+__device__ __forceinline__ void load_kmajor(unsigned char* planes, int plane_bytes, const float2* X, long ldx,
+                                            int r0, int rmax, int k0, int kend, int tid) {
+    constexpr int ITEMS = NROWS * 16 / PRODUCERS;
+    float4 v[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const int idx = tid + i * PRODUCERS;
         const int row = idx >> 4;
         const int kp = (idx & 15) * 2;  // even K offset within the block
         const int gr = r0 + row, gk = k0 + kp;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
         if (gr < rmax) {
             const float2* p = X + (long)gr * ldx + gk;
             if (gk + 1 < kend && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
-                v = *reinterpret_cast<const float4*>(p);
+                x = __ldg(reinterpret_cast<const float4*>(p));
             } else {
-                if (gk < kend) { const float2 a = p[0]; v.x = a.x; v.y = a.y; }
-                if (gk + 1 < kend) { const float2 b = p[1]; v.z = b.x; v.w = b.y; }
+                if (gk < kend) { const float2 a = __ldg(p); x.x = a.x; x.y = a.y; }
+                if (gk + 1 < kend) { const float2 b = __ldg(p + 1); x.z = b.x; x.w = b.y; }
             }
         }
-        put_pair(planes, plane_bytes, row, kp, v, conj);
+        v[i] = x;
+    }
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const int idx = tid + i * PRODUCERS;
+        put_pair(planes, plane_bytes, idx >> 4, (idx & 15) * 2, v[i], false);
     }
 }
 
 // One K block of an M-contiguous operand (A of "N,N": element (m, k) at
-// X[m + k*ldx]): each thread takes two rows and four K values.
+// X[m + k*ldx]): each item is two rows by four K values; loads first.
 __device__ __forceinline__ void load_mmajor(unsigned char* planes, int plane_bytes, const float2* X, long ldx,
                                             int m0, int mmax, int k0, int kend, int tid) {
-    for (int idx = tid; idx < (BM / 2) * (BK / 4); idx += PRODUCERS) {
+    constexpr int ITEMS = (BM / 2) * (BK / 4) / PRODUCERS;
+    float4 v[ITEMS][4];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const int idx = tid + i * PRODUCERS;
         const int mp = idx % (BM / 2);
         const int kq = idx / (BM / 2);
-        const int row = 2 * mp, gm = m0 + row;
-        float2 c0[4], c1[4];
+        const int gm = m0 + 2 * mp;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int gk = k0 + kq * 4 + j;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
             if (gk < kend && gm < mmax) {
                 const float2* p = X + (long)gk * ldx + gm;
                 if (gm + 1 < mmax && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
-                    v = *reinterpret_cast<const float4*>(p);
+                    x = __ldg(reinterpret_cast<const float4*>(p));
                 } else {
-                    const float2 a = p[0];
-                    v.x = a.x;
-                    v.y = a.y;
-                    if (gm + 1 < mmax) { const float2 b = p[1]; v.z = b.x; v.w = b.y; }
+                    const float2 a = __ldg(p);
+                    x.x = a.x;
+                    x.y = a.y;
+                    if (gm + 1 < mmax) { const float2 b = __ldg(p + 1); x.z = b.x; x.w = b.y; }
                 }
             }
-            c0[j] = make_float2(v.x, v.y);
-            c1[j] = make_float2(v.z, v.w);
+            v[i][j] = x;
         }
-        put_quad(planes, plane_bytes, row, kq * 4, c0);
-        put_quad(planes, plane_bytes, row + 1, kq * 4, c1);
+    }
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const int idx = tid + i * PRODUCERS;
+        const int mp = idx % (BM / 2);
+        const int kq = idx / (BM / 2);
+        float2 c0[4], c1[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            c0[j] = make_float2(v[i][j].x, v[i][j].y);
+            c1[j] = make_float2(v[i][j].z, v[i][j].w);
+        }
+        put_quad(planes, plane_bytes, 2 * mp, kq * 4, c0);
+        put_quad(planes, plane_bytes, 2 * mp + 1, kq * 4, c1);
+    }
+}
+
+// One K block of B (K-contiguous columns) into the two stacked planes: the
+// real parts of column n go to row n of the (hi, lo) planes, the imaginary
+// parts to row BN + n.
+__device__ __forceinline__ void load_b(unsigned char* planes, const float2* X, long ldx, int n0, int nmax,
+                                       int k0, int kend, int tid) {
+    constexpr int ITEMS = BN * 16 / PRODUCERS;
+    float4 v[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const int idx = tid + i * PRODUCERS;
+        const int row = idx >> 4;
+        const int kp = (idx & 15) * 2;
+        const int gr = n0 + row, gk = k0 + kp;
+        float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (gr < nmax) {
+            const float2* p = X + (long)gr * ldx + gk;
+            if (gk + 1 < kend && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
+                x = __ldg(reinterpret_cast<const float4*>(p));
+            } else {
+                if (gk < kend) { const float2 a = __ldg(p); x.x = a.x; x.y = a.y; }
+                if (gk + 1 < kend) { const float2 b = __ldg(p + 1); x.z = b.x; x.w = b.y; }
+            }
+        }
+        v[i] = x;
+    }
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const int idx = tid + i * PRODUCERS;
+        const int row = idx >> 4, k = (idx & 15) * 2;
+        const float4 x = v[i];
+        const float rh0 = tf32_rn(x.x), rh1 = tf32_rn(x.z), ih0 = tf32_rn(x.y), ih1 = tf32_rn(x.w);
+        const float rl0 = tf32_rn(x.x - rh0), rl1 = tf32_rn(x.z - rh1);
+        const float il0 = tf32_rn(x.y - ih0), il1 = tf32_rn(x.w - ih1);
+        const uint32_t orr = swz(row, k), oi = swz(BN + row, k);
+        *reinterpret_cast<float2*>(planes + orr) = make_float2(rh0, rh1);
+        *reinterpret_cast<float2*>(planes + B_PLANE + orr) = make_float2(rl0, rl1);
+        *reinterpret_cast<float2*>(planes + oi) = make_float2(ih0, ih1);
+        *reinterpret_cast<float2*>(planes + B_PLANE + oi) = make_float2(il0, il1);
     }
 }
 
@@ -274,19 +343,17 @@ cgemm_tc_kernel(int M, int N, int K, float2 alpha, const float2* __restrict__ A,
             unsigned char* pb = st + 4 * A_PLANE;
             const int k0 = kbeg + kb * BK;
             if (CONJ_A)
-                load_kmajor(pa, A_PLANE, BM, A, lda, m0, M, k0, kend, false, tid);
+                load_kmajor<BM>(pa, A_PLANE, A, lda, m0, M, k0, kend, tid);
             else
                 load_mmajor(pa, A_PLANE, A, lda, m0, M, k0, kend, tid);
-            load_kmajor(pb, B_PLANE, BN, B, ldb, n0, N, k0, kend, false, tid);
+            load_b(pb, B, ldb, n0, N, k0, kend, tid);
             fence_async_smem();
             mbar_arrive(&full_bar[s]);
         }
     } else if (lane == 0) {
         // ------------------------------------------------------- MMA issuer
-        // real products: (A plane, B plane, accumulator, negate A)
-        // C,N: Re += ar br + ai bi      Im += ar bi - ai br
-        // N,N: Re += ar br - ai bi      Im += ar bi + ai br
-        bool first_re = true, first_im = true;
+        // per K step: P += Ar [Br|Bi]^T, Q += Ai [Br|Bi]^T, each as hi*hi + hi*lo + lo*hi
+        bool first = true;
         bool ok = true;
         for (int kb = 0; kb < nkb && ok; ++kb) {
             const int s = kb % STAGES;
@@ -301,24 +368,17 @@ cgemm_tc_kernel(int M, int N, int K, float2 alpha, const float2* __restrict__ A,
             for (int ks = 0; ks < BK / 8; ++ks) {
                 const uint32_t off = ks * 32;
 #pragma unroll
-                for (int t = 0; t < 12; ++t) {
-                    const int prod = t / 3;           // 0: r*r 1: i*i 2: r*i 3: i*r
-                    const int term = t % 3;           // 0: hi*hi 1: hi*lo 2: lo*hi
-                    const int ap = (prod == 0 || prod == 2) ? 0 : 2;
-                    const int bp = (prod == 0 || prod == 3) ? 0 : 2;
-                    const int a_plane = ap + (term == 2 ? 1 : 0);
-                    const int b_plane = bp + (term == 1 ? 1 : 0);
-                    const bool to_im = prod >= 2;
-                    bool neg;
-                    if (CONJ_A) neg = (prod == 3);
-                    else neg = (prod == 1);
+                for (int t = 0; t < 6; ++t) {
+                    const int part = t / 3;   // 0: P (A re planes), 1: Q (A im planes)
+                    const int term = t % 3;   // 0: hi*hi 1: hi*lo 2: lo*hi
+                    const int a_plane = 2 * part + (term == 2 ? 1 : 0);
+                    const int b_plane = (term == 1 ? 1 : 0);
                     const uint64_t ad = smem_desc(a_base + a_plane * A_PLANE + off);
                     const uint64_t bd = smem_desc(b_base + b_plane * B_PLANE + off);
-                    const uint32_t d = tmem + (to_im ? BN : 0);
-                    bool& first = to_im ? first_im : first_re;
-                    mma_tf32(d, ad, bd, instr_desc(neg), first ? 0u : 1u);
-                    first = false;
+                    const uint32_t d = tmem + (part ? UMMA_N : 0);
+                    mma_tf32(d, ad, bd, instr_desc(), (first && term == 0) ? 0u : 1u);
                 }
+                first = false;
             }
             mma_commit(&empty_bar[s]);
         }
@@ -333,22 +393,25 @@ cgemm_tc_kernel(int M, int N, int K, float2 alpha, const float2* __restrict__ A,
         const int row = m0 + warp * 32 + lane;
         const uint32_t lane_addr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
         const bool use_beta = (beta.x != 0.f || beta.y != 0.f);
-#pragma unroll
+#pragma unroll 1
         for (int c0 = 0; c0 < BN; c0 += 16) {
-            float re[16], im[16];
+            float pr[16], pi[16], qr[16], qi[16];
             if (have) {
-                tmem_ld16(lane_addr + c0, re);
-                tmem_ld16(lane_addr + BN + c0, im);
+                tmem_ld16(lane_addr + c0, pr);                  // Ar Br
+                tmem_ld16(lane_addr + BN + c0, pi);             // Ar Bi
+                tmem_ld16(lane_addr + UMMA_N + c0, qr);         // Ai Br
+                tmem_ld16(lane_addr + UMMA_N + BN + c0, qi);    // Ai Bi
             } else {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) re[j] = im[j] = 0.f;
+                for (int j = 0; j < 16; ++j) pr[j] = pi[j] = qr[j] = qi[j] = 0.f;
             }
             if (row < M) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     const int col = n0 + c0 + j;
                     if (col >= N) break;
-                    const float2 acc = make_float2(re[j], im[j]);
+                    const float2 acc = CONJ_A ? make_float2(pr[j] + qi[j], pi[j] - qr[j])
+                                              : make_float2(pr[j] - qi[j], pi[j] + qr[j]);
                     if (part) {
                         part[(long)blockIdx.z * M * N + (long)col * M + row] = acc;
                     } else {
@@ -396,9 +459,10 @@ __global__ void splitk_sum(int M, int N, int splits, const float2* __restrict__ 
     }
 }
 
+// one block per SM: keep tiles x splits within one wave of 148
 int choose_splits(int M, int N, int K) {
     const int tiles = ceil_div(M, BM) * ceil_div(N, BN);
-    int s = ceil_div(148, tiles);
+    int s = 148 / tiles;
     const int kmax = ceil_div(K, 256);
     if (s > kmax) s = kmax;
     if (s < 1) s = 1;

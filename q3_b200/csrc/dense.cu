@@ -14,6 +14,7 @@
 //         Sturm counts (one warp per eigenvalue), eigenvectors by inverse
 //         iteration with Gram-Schmidt inside clusters of close eigenvalues,
 //         then the reflectors applied back (one warp per vector).
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -278,30 +279,48 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // ------------------------------------------------------------------ hetrd
-// A (n x n, ld n, full Hermitian) reduced to tridiagonal form by reflectors
-// H_k = I - tau_k v_k v_k^H acting on rows/columns k+1..n-1:
-//   d[k] = A_kk, e[k] = T(k+1, k) (complex), v_k in Vh[:, k] (rows k+1..), tau[k].
-// Column i of the trailing matrix belongs to warp (i mod total warps).
-// Data other blocks write is read with ld.global.cg (L2), never from L1.
+// A (n x n, ld n, full Hermitian; read once) reduced to tridiagonal form by
+// reflectors H_k = I - tau_k v_k v_k^H on rows/columns k+1..n-1, with
+//   d[k] = A_kk,  e[k] = T(k+1, k) (complex),  W = Q^H = H_{n-2} ... H_0,
+// so that A = Q T Q^H and an eigenvector of A is W^H times one of T.
+// Block b owns columns c = b + G*j (cyclic, G = gridDim.x); it keeps them in
+// shared memory for the whole reduction, and its columns of W too when they
+// fit (`w_in_smem`), else in global memory.  Per column step, two grid
+// barriers: one after every block has published its entries of p = tau A v
+// and its share of v^H p, one after the owner of column k+1 has updated and
+// published it.  Only that column, p and the shares cross blocks, through L2
+// (ld.global.cg); every wait is bounded.
 __global__ void __launch_bounds__(256)
-hetrd_coop(int n, double2* A, double* d, double2* e, double2* Vh, double* tau, double2* pbuf,
-           double2* partial, unsigned* bar, int* err) {
+hetrd_smem(int n, int cpb, int w_in_smem, const double2* A, double* d, double2* e, double2* W,
+           double2* xbuf, double2* pbuf, double2* partial, unsigned* bar, int* err) {
     extern __shared__ __align__(16) unsigned char smem[];
-    double2* sv = reinterpret_cast<double2*>(smem);
-    double2* sw = sv + n;
+    double2* cols = reinterpret_cast<double2*>(smem);   // cpb columns of A
+    double2* sv = cols + (size_t)cpb * n;              // v
+    double2* sw = sv + n;                              // w
+    double2* wsm = sw + n;                             // cpb columns of W (if w_in_smem)
     __shared__ double red[8];
     __shared__ double2 redc[8];
     __shared__ double s_tau;
-    __shared__ double2 s_alpha, s_x0;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int gw = blockIdx.x * 8 + warp;
-    const int nw = gridDim.x * 8;
+    const int G = gridDim.x, b = blockIdx.x;
+    const int owned = b < n ? (n - b + G - 1) / G : 0;
+    auto wcol = [&](int jj) -> double2* { return w_in_smem ? wsm + (size_t)jj * n : W + (size_t)(b + G * jj) * n; };
+    for (int jj = 0; jj < owned; ++jj) {
+        const int c = b + G * jj;
+        double2* wc = wcol(jj);
+        for (int r = tid; r < n; r += blockDim.x) {
+            cols[(size_t)jj * n + r] = A[r + (size_t)c * n];
+            wc[r] = (r == c) ? mk(1.0, 0.0) : mk(0.0, 0.0);
+        }
+    }
+    if (b == 0)
+        for (int r = tid; r < n; r += blockDim.x) xbuf[r] = A[r];
+    if (!grid_sync(bar, G, err)) return;
     for (int k = 0; k + 1 < n; ++k) {
         const int m = n - k - 1;
-        // x = A[k+1:, k]
         double part = 0.0;
         for (int j = tid; j < m; j += blockDim.x) {
-            const double2 x = __ldcg(&A[(k + 1 + j) + (long)k * n]);
+            const double2 x = __ldcg(&xbuf[k + 1 + j]);
             sv[j] = x;
             if (j > 0) part += x.x * x.x + x.y * x.y;
         }
@@ -323,28 +342,24 @@ hetrd_coop(int n, double2* A, double* d, double2* e, double2* Vh, double* tau, d
                 sv[0] = v0;
             }
             s_tau = t;
-            s_alpha = alpha;
-            s_x0 = x0;
-            if (blockIdx.x == 0) {
-                d[k] = __ldcg(&A[k + (long)k * n]).x;
+            if (b == 0) {
+                d[k] = __ldcg(&xbuf[k]).x;
                 e[k] = alpha;
-                tau[k] = t;
             }
         }
         __syncthreads();
         const double tk = s_tau;
-        if (blockIdx.x == 0) {
-            for (int j = tid; j < m; j += blockDim.x) Vh[(k + 1 + j) + (long)k * n] = tk != 0.0 ? sv[j] : mk(0.0, 0.0);
-        }
-        // p_i = tau * (column i)^H v for owned columns; partial v^H p
+        // p_i = tau (column i)^H v for the owned columns i > k; this block's share of v^H p
         double2 acc = mk(0.0, 0.0);
         if (tk != 0.0) {
-            for (int i = k + 1 + ((gw - (k + 1)) % nw + nw) % nw; i < n; i += nw) {
-                double2 s = mk(0.0, 0.0);
-                const double2* col = A + (long)i * n + (k + 1);
-                for (int j = lane; j < m; j += 32) s = s + cmulc(__ldcg(&col[j]), sv[j]);
-                s = warp_sum(s);
-                const double2 p = mk(tk * s.x, tk * s.y);
+            for (int jj = warp; jj < owned; jj += 8) {
+                const int i = b + G * jj;
+                if (i <= k) continue;
+                const double2* col = cols + (size_t)jj * n + (k + 1);
+                double2 sacc = mk(0.0, 0.0);
+                for (int j = lane; j < m; j += 32) sacc = sacc + cmulc(col[j], sv[j]);
+                sacc = warp_sum(sacc);
+                const double2 p = mk(tk * sacc.x, tk * sacc.y);
                 if (lane == 0) pbuf[i] = p;
                 acc = acc + cmulc(sv[i - k - 1], p);
             }
@@ -352,16 +367,16 @@ hetrd_coop(int n, double2* A, double* d, double2* e, double2* Vh, double* tau, d
         if (lane == 0) redc[warp] = acc;
         __syncthreads();
         if (tid == 0) {
-            double2 s = mk(0.0, 0.0);
-            for (int q = 0; q < 8; ++q) s = s + redc[q];
-            partial[blockIdx.x] = s;
+            double2 sacc = mk(0.0, 0.0);
+            for (int q = 0; q < 8; ++q) sacc = sacc + redc[q];
+            partial[b] = sacc;
         }
-        if (!grid_sync(bar, gridDim.x, err)) return;
+        if (!grid_sync(bar, G, err)) return;
         if (tk != 0.0) {
             if (tid == 0) {
-                double2 s = mk(0.0, 0.0);
-                for (int b = 0; b < (int)gridDim.x; ++b) s = s + __ldcg(&partial[b]);
-                redc[0] = s;
+                double2 sacc = mk(0.0, 0.0);
+                for (int q = 0; q < G; ++q) sacc = sacc + __ldcg(&partial[q]);
+                redc[0] = sacc;
             }
             __syncthreads();
             const double half = 0.5 * tk * redc[0].x;  // v^H p is real
@@ -370,48 +385,111 @@ hetrd_coop(int n, double2* A, double* d, double2* e, double2* Vh, double* tau, d
                 sw[j] = mk(p.x - half * sv[j].x, p.y - half * sv[j].y);
             }
             __syncthreads();
-            for (int i = k + 1 + ((gw - (k + 1)) % nw + nw) % nw; i < n; i += nw) {
+            for (int jj = warp; jj < owned; jj += 8) {
+                const int i = b + G * jj;
+                // W column: W[k+1:, i'] -= tau v (v^H W[k+1:, i'])
+                double2* wc = wcol(jj) + (k + 1);
+                double2 sacc = mk(0.0, 0.0);
+                for (int j = lane; j < m; j += 32) sacc = sacc + cmulc(sv[j], wc[j]);
+                sacc = warp_sum(sacc);
+                const double2 f = mk(tk * sacc.x, tk * sacc.y);
+                for (int j = lane; j < m; j += 32) wc[j] = wc[j] - cmul(sv[j], f);
+                if (i <= k) continue;
+                // A[j, i] -= v_j conj(w_i) + w_j conj(v_i)
                 const double2 vi = sv[i - k - 1], wi = sw[i - k - 1];
-                double2* col = A + (long)i * n + (k + 1);
+                double2* col = cols + (size_t)jj * n + (k + 1);
                 for (int j = lane; j < m; j += 32) {
-                    // A[j, i] -= v_j conj(w_i) + w_j conj(v_i)
-                    const double2 a = __ldcg(&col[j]);
                     const double2 u = cmul(sv[j], conj2(wi)) + cmul(sw[j], conj2(vi));
-                    col[j] = a - u;
+                    col[j] = col[j] - u;
                 }
             }
         }
-        if (!grid_sync(bar, gridDim.x, err)) return;
+        __syncthreads();
+        // the owner of column k+1 publishes its rows k+1.. for the next step
+        if ((k + 1) % G == b) {
+            const double2* col = cols + (size_t)((k + 1) / G) * n;
+            for (int r = k + 1 + tid; r < n; r += blockDim.x) xbuf[r] = col[r];
+        }
+        if (!grid_sync(bar, G, err)) return;
     }
-    if (blockIdx.x == 0 && tid == 0) {
-        d[n - 1] = __ldcg(&A[(n - 1) + (long)(n - 1) * n]).x;
+    if (b == 0 && tid == 0) {
+        d[n - 1] = __ldcg(&xbuf[n - 1]).x;
         e[n - 1] = mk(0.0, 0.0);
-        tau[n - 1] = 0.0;
+    }
+    if (w_in_smem) {
+        for (int jj = 0; jj < owned; ++jj) {
+            const int c = b + G * jj;
+            for (int r = tid; r < n; r += blockDim.x) W[r + (size_t)c * n] = wsm[(size_t)jj * n + r];
+        }
     }
 }
 
-// |e|, e^2, the phases delta_{k+1} = delta_k e_k/|e_k| and Gershgorin bounds
+// |e|, e^2, Gershgorin bounds and the phases delta_{k+1} = delta_k e_k/|e_k|
+// (a prefix product: one warp, chunks of the vector per lane, a shuffle scan
+// across lanes)
 __global__ void tridiag_prep(int n, const double* d, const double2* e, double* ea, double* e2,
                              double2* phase, double* bounds) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double2 ph = mk(1.0, 0.0);
+    const int lane = threadIdx.x;
+    if (blockIdx.x != 0 || lane >= 32) return;
+    const int chunk = (n + 31) / 32;
+    const int k0 = lane * chunk, k1 = min(n, k0 + chunk);
     double lo = 1e300, hi = -1e300;
-    for (int k = 0; k < n; ++k) {
-        phase[k] = ph;
+    for (int k = k0; k < k1; ++k) {
         const double a = (k + 1 < n) ? hypot(e[k].x, e[k].y) : 0.0;
         if (k + 1 < n) {
             ea[k] = a;
             e2[k] = a * a;
-            if (a > 0.0) ph = cmul(ph, mk(e[k].x / a, e[k].y / a));
         }
-        const double left = (k > 0) ? ea[k - 1] : 0.0;
+        const double left = (k > 0) ? hypot(e[k - 1].x, e[k - 1].y) : 0.0;
         lo = fmin(lo, d[k] - left - a);
         hi = fmax(hi, d[k] + left + a);
     }
-    const double scale = fmax(fabs(lo), fabs(hi));
-    bounds[0] = lo - 4.0 * 2.220446049250313e-16 * scale - 1e-300;
-    bounds[1] = hi + 4.0 * 2.220446049250313e-16 * scale + 1e-300;
-    bounds[2] = scale;
+    // product of the unit factors u_k = e_k/|e_k| over this lane's chunk
+    double2 prod = mk(1.0, 0.0);
+    for (int k = k0; k < k1 && k + 1 < n; ++k) {
+        const double a = hypot(e[k].x, e[k].y);
+        if (a > 0.0) prod = cmul(prod, mk(e[k].x / a, e[k].y / a));
+    }
+    // exclusive scan of the chunk products across lanes
+    double2 incl = prod;
+    for (int o = 1; o < 32; o <<= 1) {
+        double2 t;
+        t.x = __shfl_up_sync(0xffffffffu, incl.x, o);
+        t.y = __shfl_up_sync(0xffffffffu, incl.y, o);
+        if (lane >= o) incl = cmul(t, incl);
+    }
+    double2 ph;
+    ph.x = __shfl_up_sync(0xffffffffu, incl.x, 1);
+    ph.y = __shfl_up_sync(0xffffffffu, incl.y, 1);
+    if (lane == 0) ph = mk(1.0, 0.0);
+    for (int k = k0; k < k1; ++k) {
+        phase[k] = ph;
+        if (k + 1 < n) {
+            const double a = hypot(e[k].x, e[k].y);
+            if (a > 0.0) ph = cmul(ph, mk(e[k].x / a, e[k].y / a));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (lane == 0) {
+        const double scale = fmax(fabs(lo), fabs(hi));
+        bounds[0] = lo - 4.0 * 2.220446049250313e-16 * scale - 1e-300;
+        bounds[1] = hi + 4.0 * 2.220446049250313e-16 * scale + 1e-300;
+        bounds[2] = scale;
+    }
+}
+
+// Yc[:, c] = phase .* Y[:, c] (complex)
+__global__ void apply_phase(int n, int nvec, const double2* phase, const double* Y, double2* Yc) {
+    const long total = (long)n * nvec;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const int r = static_cast<int>(t % n);
+        const double2 p = phase[r];
+        const double y = Y[t];
+        Yc[t] = mk(p.x * y, p.y * y);
+    }
 }
 
 // number of eigenvalues of the real tridiagonal (d, e2) below x
@@ -451,14 +529,16 @@ __global__ void tridiag_multisect(int n, const double* d, const double* e2, cons
     if (lane == 0) w[i] = 0.5 * (a + b);
 }
 
-// Inverse iteration, one thread per cluster of close eigenvalues (gap below
-// 1e-3 * ||T||, as LAPACK's dstein groups them); Gram-Schmidt inside a cluster.
+// Inverse iteration, one thread per cluster of close eigenvalues;
+// Gram-Schmidt inside a cluster.  Vectors of eigenvalues a gap g apart come
+// out orthogonal to about eps ||T|| / g without it, so clusters are cut at a
+// gap of 1e-5 ||T|| (orthogonality ~1e-11 across clusters).
 __global__ void tridiag_invit(int n, const double* d, const double* ea, const double* w,
                               const double* bounds, int nvec, double* Y, double* work) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nvec) return;
     const double scale = fmax(bounds[2], 1e-300);
-    const double ortol = 1e-3 * scale;
+    const double ortol = 1e-5 * scale;
     if (i > 0 && w[i] - w[i - 1] <= ortol) return;
     int jend = i + 1;
     while (jend < nvec && w[jend] - w[jend - 1] <= ortol) ++jend;
@@ -535,33 +615,6 @@ __global__ void tridiag_invit(int n, const double* d, const double* ea, const do
     }
 }
 
-// Z[:, c] = Q (phase .* Y[:, c]), Q = H_0 H_1 ... H_{n-2}; one warp per column
-__global__ void herm_backtransform(int n, int nvec, const double2* Vh, const double* tau,
-                                   const double2* phase, const double* Y, double2* Z) {
-    const int lane = threadIdx.x & 31;
-    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (c >= nvec) return;
-    double2* z = Z + (long)c * n;
-    const double* y = Y + (long)c * n;
-    for (int r = lane; r < n; r += 32) {
-        const double2 p = phase[r];
-        z[r] = mk(p.x * y[r], p.y * y[r]);
-    }
-    __syncwarp();
-    for (int k = n - 2; k >= 0; --k) {
-        const double t = tau[k];
-        if (t == 0.0) continue;
-        const int m = n - k - 1;
-        const double2* v = Vh + (long)k * n + (k + 1);
-        double2 s = mk(0.0, 0.0);
-        for (int j = lane; j < m; j += 32) s = s + cmulc(v[j], z[k + 1 + j]);
-        s = warp_sum(s);
-        s = mk(t * s.x, t * s.y);
-        for (int j = lane; j < m; j += 32) z[k + 1 + j] = z[k + 1 + j] - cmul(v[j], s);
-        __syncwarp();
-    }
-}
-
 struct Chol {
     double2* dinv;
     int* info;
@@ -614,12 +667,12 @@ size_t potrf_scratch_bytes(int n) {
 }
 
 size_t hegv_scratch_bytes(int n) {
-    // slices taken by hegv + heev: five n x n complex matrices (and the
-    // n x nvec eigenvector block), an n x n real block plus five more for
-    // inverse iteration, a few length-n vectors, and 256-byte alignment slack
+    // hegv: U, U^-1, H, H U^-1 (n x n complex each) and the eigenvector block;
+    // heev: W (n x n complex), Y and D Y, five real work vectors per
+    // eigenvector; a few length-n vectors; 256-byte alignment slack
     const size_t nn = (size_t)n * n;
-    return potrf_scratch_bytes(n) + 6 * nn * sizeof(double2) + 6 * nn * sizeof(double) +
-           64 * (size_t)n * sizeof(double2) + 64 * 1024;
+    return potrf_scratch_bytes(n) + 5 * nn * sizeof(double2) + nn * (sizeof(double2) + 6 * sizeof(double)) +
+           nn * sizeof(double2) + 64 * (size_t)n * sizeof(double2) + 64 * 1024;
 }
 
 int potrf(cudaStream_t st, int n, double2* A, int lda, Scratch& ws) {
@@ -632,43 +685,50 @@ void trtri_after_potrf(cudaStream_t st, int n, const double2* A, int lda, double
     trtri_impl(st, n, A, lda, c, Uinv);
 }
 
-void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, Scratch& ws) {
+void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, Scratch& ws,
+          const GemmWorkspace& gws) {
     if (n <= 0) return;
+    const int nv = nvec > 0 ? nvec : 1;
     double* d = ws.take<double>(n);
     double2* e = ws.take<double2>(n);
-    double* tau = ws.take<double>(n);
-    double2* Vh = ws.take<double2>((size_t)n * n);
+    double2* W = ws.take<double2>((size_t)n * n);
+    double2* xbuf = ws.take<double2>(n);
     double2* pbuf = ws.take<double2>(n);
     double* ea = ws.take<double>(n);
     double* e2 = ws.take<double>(n);
     double2* phase = ws.take<double2>(n);
     double* bounds = ws.take<double>(4);
-    double* Y = ws.take<double>((size_t)n * (nvec > 0 ? nvec : 1));
-    double* work = ws.take<double>((size_t)5 * n * (nvec > 0 ? nvec : 1));
+    double* Y = ws.take<double>((size_t)n * nv);
+    double* work = ws.take<double>((size_t)5 * n * nv);
+    double2* Yc = ws.take<double2>((size_t)n * nv);
     int device = 0;
     Q3B_CUDA(cudaGetDevice(&device));
     int nsm = 0;
     Q3B_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-    int blocks = ceil_div(n, 8);
-    if (blocks > nsm) blocks = nsm;
-    if (blocks < 1) blocks = 1;
-    double2* partial = ws.take<double2>(blocks);
+    // blocks: about 8 columns each, at most one per SM; columns (and W) in shared memory
+    int G = std::max(1, std::min(nsm, (n + 7) / 8));
+    int cpb = (n + G - 1) / G;
+    const size_t limit = 200 * 1024;
+    size_t smem = ((size_t)cpb * n + 2 * (size_t)n) * sizeof(double2);
+    if (smem > limit) throw Status(Q3B_ERR_INVALID, "subspace of order " + std::to_string(n) + " too large for the eigensolver");
+    int w_in_smem = (smem + (size_t)cpb * n * sizeof(double2) <= limit) ? 1 : 0;
+    if (w_in_smem) smem += (size_t)cpb * n * sizeof(double2);
+    double2* partial = ws.take<double2>(G);
     unsigned* bar = ws.take<unsigned>(2);
     int* err = ws.take<int>(1);
     Q3B_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
     Q3B_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
-    Q3B_CUDA(cudaMemsetAsync(Vh, 0, (size_t)n * n * sizeof(double2), st));
-    const size_t smem = 2 * (size_t)n * sizeof(double2);
     static bool attr_set = false;
     if (!attr_set) {
-        Q3B_CUDA(cudaFuncSetAttribute(hetrd_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        Q3B_CUDA(cudaFuncSetAttribute(hetrd_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit));
         attr_set = true;
     }
     int per_sm = 0;
-    Q3B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_coop, 256, smem));
-    if (per_sm < 1) throw Status(Q3B_ERR_INVALID, "subspace too large for the eigensolver");
-    void* args[] = {&n, &A, &d, &e, &Vh, &tau, &pbuf, &partial, &bar, &err};
-    Q3B_CUDA(cudaLaunchCooperativeKernel((const void*)hetrd_coop, dim3(blocks), dim3(256), args, smem, st));
+    Q3B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_smem, 256, smem));
+    if (per_sm < 1 || per_sm * nsm < G) throw Status(Q3B_ERR_INVALID, "eigensolver blocks cannot be co-resident");
+    const double2* Ac = A;
+    void* args[] = {&n, &cpb, &w_in_smem, &Ac, &d, &e, &W, &xbuf, &pbuf, &partial, &bar, &err};
+    Q3B_CUDA(cudaLaunchCooperativeKernel((const void*)hetrd_smem, dim3(G), dim3(256), args, smem, st));
     Q3B_LAUNCH_CHECK();
     tridiag_prep<<<1, 32, 0, st>>>(n, d, e, ea, e2, phase, bounds);
     Q3B_LAUNCH_CHECK();
@@ -677,8 +737,10 @@ void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, S
     if (nvec > 0) {
         tridiag_invit<<<ceil_div(nvec, 64), 64, 0, st>>>(n, d, ea, w, bounds, nvec, Y, work);
         Q3B_LAUNCH_CHECK();
-        herm_backtransform<<<ceil_div((long)nvec * 32, 256), 256, 0, st>>>(n, nvec, Vh, tau, phase, Y, Z);
+        apply_phase<<<grid_for((long)n * nvec), 256, 0, st>>>(n, nvec, phase, Y, Yc);
         Q3B_LAUNCH_CHECK();
+        const double2 one = mk(1.0, 0.0), zero = mk(0.0, 0.0);
+        cgemm<double>(st, true, n, nvec, n, one, W, n, Yc, n, zero, Z, n, gws);   // Z = W^H (D Y)
     }
     int herr = 0;
     Q3B_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -709,7 +771,7 @@ int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, dou
     hermitian_from_upper<<<grid_for((long)nn), 256, 0, st>>>(n, Hf, n, W);
     Q3B_LAUNCH_CHECK();
     double2* Zc = ws.take<double2>((size_t)n * (nvec > 0 ? nvec : 1));
-    heev(st, n, W, w, Zc, nvec, ws);
+    heev(st, n, W, w, Zc, nvec, ws, gws);
     if (nvec > 0) cgemm<double>(st, false, n, nvec, n, one, Ui, n, Zc, n, zero, Z, n, gws);
     return 0;
 }

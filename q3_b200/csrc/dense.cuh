@@ -48,9 +48,10 @@ int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, dou
          int nvec, Scratch& ws, const GemmWorkspace& gws);
 
 // Standard Hermitian eigenproblem of a full (both triangles) matrix A (n x n,
-// ld n; destroyed).  Eigenvalues ascending in w, the first nvec eigenvectors
+// ld n; read only).  Eigenvalues ascending in w, the first nvec eigenvectors
 // in Z (ld n).
-void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, Scratch& ws);
+void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, Scratch& ws,
+          const GemmWorkspace& gws);
 
 }  // namespace dense
 }  // namespace q3b
