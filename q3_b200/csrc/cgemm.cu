@@ -161,7 +161,7 @@ template <typename R> int choose_splits(int M, int N, int K) {
     const int tiles = ceil_div(M, kBM) * ceil_div(N, kBN);
     const int target = 2 * 148;
     int s = ceil_div(target, tiles);
-    const int kmax = ceil_div(K, 512);
+    const int kmax = ceil_div(K, 128);
     if (s > kmax) s = kmax;
     if (s < 1) s = 1;
     if (s > 64) s = 64;

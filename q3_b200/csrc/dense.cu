@@ -31,62 +31,56 @@ constexpr int NB = 32;
 __device__ __forceinline__ int vload(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
 
 // ------------------------------------------------------------------ potrf
-__global__ void __launch_bounds__(256)
+// Diagonal block k: one warp factors the 32x32 block (lane c owns column c)
+// and inverts the triangular factor (lane c computes column c of U^-1).
+__global__ void __launch_bounds__(32)
 potrf_diag(int n, int k, double2* A, int lda, double2* dinv, int* info) {
     if (vload(info)) return;
     __shared__ double2 a[NB][NB + 1];  // a[c][r] = element (r, c)
     __shared__ double2 x[NB][NB + 1];
-    __shared__ int bad;
     const int r0 = k * NB;
     const int bs = min(NB, n - r0);
-    const int tid = threadIdx.x;
-    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-        const int r = idx % NB, c = idx / NB;
+    const int c = threadIdx.x;
+    for (int r = 0; r < NB; ++r) {
         double2 v = (r == c) ? mk(1.0, 0.0) : mk(0.0, 0.0);
         if (r < bs && c < bs) v = A[(r0 + r) + (long)(r0 + c) * lda];
         a[c][r] = v;
         x[c][r] = mk(0.0, 0.0);
     }
-    if (tid == 0) bad = 0;
-    __syncthreads();
+    __syncwarp();
+    int bad = 0;
     for (int j = 0; j < NB; ++j) {
-        if (tid == 0) {
-            double piv = a[j][j].x;
-            if (!(piv > 0.0)) {
-                if (!bad && j < bs) bad = r0 + j + 1;
-                piv = 1.0;
-            }
-            a[j][j] = mk(sqrt(piv), 0.0);
+        // lane j takes the pivot; every lane reads it
+        double piv = a[j][j].x;
+        if (!(piv > 0.0)) {
+            if (!bad && j < bs) bad = r0 + j + 1;
+            piv = 1.0;
         }
-        __syncthreads();
-        if (tid > j && tid < NB) {
-            const double u = a[j][j].x;
-            a[tid][j] = mk(a[tid][j].x / u, a[tid][j].y / u);
+        const double u = sqrt(piv);
+        __syncwarp();
+        if (c == j) a[j][j] = mk(u, 0.0);
+        if (c > j) a[c][j] = mk(a[c][j].x / u, a[c][j].y / u);   // U(j, c)
+        __syncwarp();
+        // trailing update of column c: G(r, c) -= conj(U(j, r)) U(j, c), j < r <= c
+        if (c > j) {
+            const double2 ujc = a[c][j];
+            for (int r = j + 1; r <= c; ++r) a[c][r] = a[c][r] - cmulc(a[r][j], ujc);
         }
-        __syncthreads();
-        for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-            const int r = idx % NB, c = idx / NB;
-            if (r > j && c >= r) a[c][r] = a[c][r] - cmulc(a[r][j], a[c][j]);
-        }
-        __syncthreads();
+        __syncwarp();
     }
-    // X = U^{-1}: column c by thread c
-    if (tid < NB) {
-        const int c = tid;
-        for (int r = c; r >= 0; --r) {
-            double2 s = (r == c) ? mk(1.0, 0.0) : mk(0.0, 0.0);
-            for (int t = r + 1; t <= c; ++t) s = s - cmul(a[t][r], x[c][t]);
-            const double u = a[r][r].x;
-            x[c][r] = mk(s.x / u, s.y / u);
-        }
+    // X = U^{-1}, column c by lane c
+    for (int r = c; r >= 0; --r) {
+        double2 s = (r == c) ? mk(1.0, 0.0) : mk(0.0, 0.0);
+        for (int t = r + 1; t <= c; ++t) s = s - cmul(a[t][r], x[c][t]);
+        const double u = a[r][r].x;
+        x[c][r] = mk(s.x / u, s.y / u);
     }
-    __syncthreads();
-    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-        const int r = idx % NB, c = idx / NB;
+    __syncwarp();
+    for (int r = 0; r < NB; ++r) {
         if (r < bs && c < bs && r <= c) A[(r0 + r) + (long)(r0 + c) * lda] = a[c][r];
         dinv[(long)k * NB * NB + r + c * NB] = x[c][r];
     }
-    if (tid == 0 && bad) atomicCAS(info, 0, bad);
+    if (c == 0 && bad) atomicCAS(info, 0, bad);
 }
 
 // U(k, j) = U_kk^{-H} G(k, j) for every block column j > k
@@ -227,37 +221,42 @@ inline int grid_for(long n) {
 }
 
 // ------------------------------------------------------------ grid barrier
-// Arrival counter + generation word; every wait is bounded (about 2 s of
+// One monotonic arrival counter: the e-th barrier of a launch completes when
+// the counter reaches e * nblocks.  Every wait is bounded (about 2 s of
 // clock), after which the kernel records an error and all blocks leave.
+__device__ unsigned& grid_epoch() {
+    __shared__ unsigned s_epoch;
+    return s_epoch;
+}
+__device__ __forceinline__ void grid_sync_init() {
+    if (threadIdx.x == 0) grid_epoch() = 0;
+}
 __device__ __forceinline__ bool grid_sync(unsigned* bar, unsigned nblocks, int* err) {
     __shared__ int s_ok;
+    unsigned& s_epoch = grid_epoch();
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned* vgen = bar + 1;
-        const unsigned gen = *vgen;
+        const unsigned epoch = s_epoch + 1;  // barriers this block has entered
+        s_epoch = epoch;
         __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u);
+        atomicAdd(bar, 1u);
+        const unsigned target = epoch * nblocks;
         int ok = 1;
-        if (arrived == nblocks - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            const long long t0 = clock64();
-            while (*vgen == gen) {
-                if (vload(err)) {
-                    ok = 0;
-                    break;
-                }
-                if (clock64() - t0 > (1LL << 32)) {
-                    atomicExch(err, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
+        const long long t0 = clock64();
+        while (true) {
+            unsigned cur;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(bar) : "memory");
+            if (cur >= target) break;
+            if (vload(err)) {
+                ok = 0;
+                break;
+            }
+            if (clock64() - t0 > (1LL << 32)) {
+                atomicExch(err, 1);
+                ok = 0;
+                break;
             }
         }
-        __threadfence();
         s_ok = ok;
     }
     __syncthreads();
@@ -304,6 +303,7 @@ hetrd_smem(int n, int cpb, int w_in_smem, const double2* A, double* d, double2* 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int G = gridDim.x, b = blockIdx.x;
     const int owned = b < n ? (n - b + G - 1) / G : 0;
+    grid_sync_init();
     auto wcol = [&](int jj) -> double2* { return w_in_smem ? wsm + (size_t)jj * n : W + (size_t)(b + G * jj) * n; };
     for (int jj = 0; jj < owned; ++jj) {
         const int c = b + G * jj;
@@ -632,7 +632,7 @@ int potrf_impl(cudaStream_t st, int n, double2* A, int lda, const Chol& c) {
     const int nblk = ceil_div(n, NB);
     Q3B_CUDA(cudaMemsetAsync(c.info, 0, sizeof(int), st));
     for (int k = 0; k < nblk; ++k) {
-        potrf_diag<<<1, 256, 0, st>>>(n, k, A, lda, c.dinv, c.info);
+        potrf_diag<<<1, 32, 0, st>>>(n, k, A, lda, c.dinv, c.info);
         Q3B_LAUNCH_CHECK();
         const int m = nblk - k - 1;
         if (m > 0) {
