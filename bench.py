@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--impl", choices=["q3b", "reference"], default="q3b")
     ap.add_argument("--no-davidson", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--davidson-tol", type=float, default=1e-9, help="Ry")
+    ap.add_argument("--serving-requests", type=int, default=32)
+    ap.add_argument("--serving-rate", type=float, default=20.0, help="arrivals per second")
     return ap.parse_args()
 
 
@@ -216,6 +217,98 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+
+# ------------------------------------------------------------------- Davidson
+def davidson_section(ap, sy1, psi64, args):
+    """Per-iteration time on the 64-atom cell; converged solves of config 0
+    (FP64 vs mixed); the 32 k-points of config 2 and a sample of the config 4
+    request stream through the serving loop, FP64 vs mixed."""
+    import torch
+    from q3_b200 import synthetic
+    from q3_b200._lib import FP64, MIXED
+    from q3_b200.davidson import PlanewaveDavidsonDiagonalizer
+    from q3_b200.serving import BandSolveServer, run_poisson_stream
+    out = {}
+    nb = sy1.nbands
+    # (1) config 1: 12 iterations, all bands unconverged (tolerance below reach)
+    it = 12
+    d = PlanewaveDavidsonDiagonalizer(ap, FP64)
+    d.set_tolerance(1e-14)
+    d.set_maximum_iterations(it)
+    d.set_profile_stages(False)
+    r64 = d.solve(psi64.clone(), nb)
+    d = PlanewaveDavidsonDiagonalizer(ap, MIXED)
+    d.set_tolerance(1e-14)
+    d.set_maximum_iterations(it)
+    d.set_precision(MIXED, 1e-14, 1)
+    rmx = d.solve(psi64.clone(), nb)
+    ms64 = 1e3 * r64.seconds / r64.iterations
+    ms32 = 1e3 * (rmx.seconds - rmx.fp64_seconds) / max(1, rmx.iterations - rmx.fp64_iterations)
+    out["config1_iteration_ms"] = {"fp64": ms64, "mixed_fp32_phase": ms32, "ratio": ms64 / ms32,
+                                   "iterations": it, "bands": nb}
+    # (2) config 0: converged solves, tolerance 1e-10 Ry
+    sy0 = synthetic.config(0)
+    ap.update_potential(sy0.v_r, sy0.cell.grid)
+    ap.prepare_system_kpoint(sy0)
+    res = {}
+    for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+        d = PlanewaveDavidsonDiagonalizer(ap, prec)
+        d.set_tolerance(1e-10)
+        d.set_maximum_iterations(200)
+        if prec == MIXED:
+            d.set_precision(MIXED, 1e-6, 200)
+        d.solve(sy0.psi0[0], sy0.nbands)            # warm
+        reps, t0 = 5, time.perf_counter()
+        for _ in range(reps):
+            r = d.solve(sy0.psi0[0], sy0.nbands)
+        res[name] = (r, reps / (time.perf_counter() - t0))
+    out["config0_solves"] = {
+        "tolerance_ry": 1e-10,
+        "fp64": {"solves_per_s": res["fp64"][1], "iterations": res["fp64"][0].iterations},
+        "mixed": {"solves_per_s": res["mixed"][1], "iterations": res["mixed"][0].iterations,
+                  "fp64_iterations": res["mixed"][0].fp64_iterations},
+        "mixed_vs_fp64_max_eig_err_ha": float(np.max(np.abs(res["mixed"][0].eigenvalues -
+                                                            res["fp64"][0].eigenvalues))) / 2.0,
+        "speedup": res["mixed"][1] / res["fp64"][1],
+    }
+    # (3) config 2: the 32 k-points, all submitted at once to 8 workers
+    sy2 = synthetic.config(2)
+    k2 = {}
+    for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+        srv = BandSolveServer(workers=8)
+        t0 = time.perf_counter()
+        ids = [srv.submit(sy2, k=k, tolerance=1e-9, max_iterations=200, precision=prec)
+               for k in range(len(sy2.kpoints))]
+        got = [srv.wait(i) for i in ids]
+        wall = time.perf_counter() - t0
+        srv.close()
+        k2[name] = (got, wall)
+    err = max(float(np.max(np.abs(a.eigenvalues - b.eigenvalues)))
+              for a, b in zip(k2["fp64"][0], k2["mixed"][0]))
+    out["config2_kpoints"] = {
+        "kpoints": len(sy2.kpoints), "tolerance_ry": 1e-9, "workers": 8,
+        "fp64": {"kpoints_per_s": len(sy2.kpoints) / k2["fp64"][1], "wall_s": k2["fp64"][1]},
+        "mixed": {"kpoints_per_s": len(sy2.kpoints) / k2["mixed"][1], "wall_s": k2["mixed"][1]},
+        "mixed_vs_fp64_max_eig_err_ha": err / 2.0,
+        "speedup": k2["fp64"][1] / k2["mixed"][1],
+    }
+    # (4) config 4: a sample of the Poisson request stream
+    systems = synthetic.serving_requests(args.serving_requests)
+    s4 = {}
+    for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+        srv = BandSolveServer(workers=8, hbm_budget=64 << 30)
+        o = run_poisson_stream(srv, systems, rate_hz=args.serving_rate, tolerance=1e-8,
+                               max_iterations=200, precision=prec)
+        srv.close()
+        o.pop("results")
+        s4[name] = o
+    out["config4_serving"] = {"requests": len(systems), "rate_hz": args.serving_rate,
+                              "tolerance_ry": 1e-8, "fp64": s4["fp64"], "mixed": s4["mixed"]}
+    # back to the bench cell
+    ap.update_potential(sy1.v_r, sy1.cell.grid)
+    ap.prepare_system_kpoint(sy1)
+    return out
+
 # --------------------------------------------------------------------- q3b arm
 def run_q3b(args):
     import torch
@@ -332,36 +425,10 @@ def run_q3b(args):
         e2e = float(t.item())
     io_bytes = nb * kp.npw * 16
 
-    # Davidson solves, FP64 and mixed, on the same cell
+    # Davidson: per iteration on this cell; converged solves on the other configs
     dav = None
     if not args.no_davidson:
-        def solve(prec):
-            d = PlanewaveDavidsonDiagonalizer(ap, prec)
-            d.set_tolerance(args.davidson_tol)
-            d.set_maximum_iterations(100)
-            if prec == MIXED:
-                d.set_precision(MIXED, 1e-5, 12)
-            x = psi64.clone()
-            torch.cuda.synchronize()
-            r = d.solve(x, nb)
-            return r
-        r64 = solve(FP64)
-        rmx = solve(MIXED)
-        err_ry = float(np.max(np.abs(rmx.eigenvalues - r64.eigenvalues)))
-        dav = {
-            "tolerance_ry": args.davidson_tol,
-            "fp64": {"solves_per_s": world / r64.seconds, "seconds": r64.seconds,
-                     "iterations": r64.iterations, "ms_per_iteration": 1e3 * r64.seconds / max(1, r64.iterations),
-                     "h_applications": r64.h_applications, "max_residual_norm": r64.max_residual_norm,
-                     "unconverged": r64.unconverged},
-            "mixed": {"solves_per_s": world / rmx.seconds, "seconds": rmx.seconds,
-                      "iterations": rmx.iterations, "fp64_iterations": rmx.fp64_iterations,
-                      "ms_per_iteration": 1e3 * rmx.seconds / max(1, rmx.iterations),
-                      "h_applications": rmx.h_applications, "max_residual_norm": rmx.max_residual_norm,
-                      "unconverged": rmx.unconverged},
-            "mixed_vs_fp64_max_eig_err_ha": err_ry / 2.0,
-            "mixed_speedup": r64.seconds / rmx.seconds,
-        }
+        dav = davidson_section(ap, sy, psi64, args)
 
     if rank != 0:
         if pg is not None:

@@ -183,6 +183,7 @@ typedef struct {
                                     orthogonalize, hamiltonian, subspace_update, collapse,
                                     extract (the reference's DavidsonTimingAccumulator
                                     stages, counters.hpp:36-52)                             */
+    double fp64_seconds;         /* MIXED: wall time of the FP64 refinement phase           */
 } q3b_davidson_stats;
 
 void q3b_davidson_default_opts(q3b_davidson_opts* opts);
@@ -200,6 +201,54 @@ int q3b_davidson_solve(q3b_context* ctx, q3b_cplx128* bands_host, double* eigenv
 int q3b_davidson_solve_dev(q3b_context* ctx, q3b_cplx128* bands_dev, double* eigenvalues_host,
                            int nb, const q3b_davidson_opts* opts, q3b_davidson_stats* stats);
 
+/* ---- serving: continuous batching of band-solve requests ------------------- */
+
+/* A request: one cell at one k-point, everything q3b_set_potential,
+ * q3b_prepare_kpoint and q3b_davidson_solve take, all host pointers (copied at
+ * submission).  No counterpart in the reference, which solves k-points one
+ * after another from its SCF loop (iterator/.../pseudopotential/init.hpp:1059). */
+typedef struct {
+    int n1, n2, n3;
+    const double* v_r;
+    int npw;
+    const int32_t* g_to_grid;
+    const double* ke;
+    int nproj;
+    const q3b_cplx128* beta;
+    int natoms;
+    const int32_t* atom_proj_offsets;
+    const double* d_blocks;
+    int nb;
+    const q3b_cplx128* bands;        /* starting bands, npw x nb                    */
+    const double* eigenvalues;       /* stored eigenvalues, nb; NULL = none         */
+    const q3b_davidson_opts* opts;   /* NULL = q3b_davidson_default_opts            */
+} q3b_request;
+
+typedef struct {
+    double queue_ms;                 /* submission to start                        */
+    double solve_ms;                 /* start to finish                            */
+    double latency_ms;               /* submission to finish                       */
+    size_t estimated_bytes;          /* device memory charged to the HBM budget     */
+} q3b_request_times;
+
+typedef struct q3b_server q3b_server;
+
+/* A server on CUDA device `device` with `workers` concurrent solves (each its
+ * own context and stream).  A queued request starts, oldest first, when a
+ * worker is free and its memory estimate fits hbm_budget_bytes beside the
+ * running ones (0 = no budget; one request always runs). */
+int q3b_server_create(int device, size_t hbm_budget_bytes, int workers, q3b_server** out);
+int q3b_server_destroy(q3b_server* server);
+const char* q3b_server_last_error(const q3b_server* server);
+int q3b_server_submit(q3b_server* server, const q3b_request* request, int* id_out);
+/* 1 finished, 0 pending, -1 unknown id */
+int q3b_server_poll(q3b_server* server, int id);
+/* Block until request `id` is done; copy out the eigenvectors (npw x nb), the
+ * eigenvalues (nb), its statistics and times (any may be NULL) and forget it.
+ * Returns the solve's status. */
+int q3b_server_wait(q3b_server* server, int id, q3b_cplx128* bands_out, double* eigenvalues_out,
+                    q3b_davidson_stats* stats, q3b_request_times* times);
+
 /* ---- dense FP64 subspace kernels (PlanewaveSubspaceManager pieces) ---------- */
 
 /* diagonalize_subspace (subspace_manager/init.hpp:82; subspace/serial.hpp:18-151):
@@ -210,6 +259,34 @@ int q3b_davidson_solve_dev(q3b_context* ctx, q3b_cplx128* bands_dev, double* eig
  * not positive definite. */
 int q3b_hegv(q3b_context* ctx, int n, const q3b_cplx128* h_dev, const q3b_cplx128* s_dev, int ld,
              double* w_dev, q3b_cplx128* evec_dev);
+
+/* ---- starting-subspace rotation (StartingSubspaceSolver) -------------------- */
+
+/* The three large steps of the starting rotation of one k-point's bands
+ * (wavefunction/planewave/starting_subspace_solver.hpp:29-59, driven by
+ * wavefunction/planewave/norm_conserving/initializer.hpp:250-385), FP64, on
+ * the context's prepared k-point; the overlap is the identity (norm-conserving).
+ *
+ * apply_hamiltonian: copy the nchi starting vectors chi (host, npw x nchi,
+ * column-major) to the device and apply H; chi and H chi stay on the device
+ * for the two calls below. */
+int q3b_start_apply(q3b_context* ctx, const q3b_cplx128* chi_host, int nchi);
+/* project: H_ij = chi_i^H (H chi)_j and S_ij = chi_i^H chi_j, each nchi x nchi,
+ * column-major, into host arrays. */
+int q3b_start_project(q3b_context* ctx, q3b_cplx128* h_host, q3b_cplx128* s_host);
+/* rotate_into_bands: band n = chi (column n of coefficients), coefficients on
+ * the host (nchi x nb, ld nchi), bands written to DEVICE memory (npw x nb), as
+ * the reference stores them in the quantum system's device block: only the
+ * coefficients cross to the device. */
+int q3b_start_rotate(q3b_context* ctx, const q3b_cplx128* coefficients_host, int nb,
+                     q3b_cplx128* bands_dev);
+/* The whole rotation on the device: q3b_start_apply, the projections, the
+ * generalized problem (zhegv itype 1 on the upper triangles, as the
+ * initializer calls it), bands = chi c[:, :nb] into bands_dev and the nb
+ * lowest eigenvalues (Ry) into eigenvalues_host.  Returns Q3B_ERR_LINALG when
+ * the starting vectors' overlap is not positive definite. */
+int q3b_starting_subspace(q3b_context* ctx, const q3b_cplx128* chi_host, int nchi, int nb,
+                          q3b_cplx128* bands_dev, double* eigenvalues_host);
 
 #ifdef __cplusplus
 }

@@ -57,10 +57,24 @@ class DavidsonStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("fp64_iterations", C.c_int),
                 ("h_applications", C.c_int), ("unconverged", C.c_int), ("collapses", C.c_int),
                 ("max_residual_norm", C.c_double), ("seconds", C.c_double),
-                ("stage_ms", C.c_double * 8)]
+                ("stage_ms", C.c_double * 8), ("fp64_seconds", C.c_double)]
 
     STAGES = ("seed", "diagonalize", "correction", "orthogonalize", "hamiltonian",
               "subspace_update", "collapse", "extract")
+
+
+class Request(C.Structure):
+    _fields_ = [("n1", C.c_int), ("n2", C.c_int), ("n3", C.c_int), ("v_r", C.c_void_p),
+                ("npw", C.c_int), ("g_to_grid", C.c_void_p), ("ke", C.c_void_p),
+                ("nproj", C.c_int), ("beta", C.c_void_p), ("natoms", C.c_int),
+                ("atom_proj_offsets", C.c_void_p), ("d_blocks", C.c_void_p), ("nb", C.c_int),
+                ("bands", C.c_void_p), ("eigenvalues", C.c_void_p),
+                ("opts", C.POINTER(DavidsonOpts))]
+
+
+class RequestTimes(C.Structure):
+    _fields_ = [("queue_ms", C.c_double), ("solve_ms", C.c_double), ("latency_ms", C.c_double),
+                ("estimated_bytes", C.c_size_t)]
 
 
 _vp, _i, _d, _sz = C.c_void_p, C.c_int, C.c_double, C.c_size_t
@@ -92,6 +106,16 @@ SIGNATURES = {
     "q3b_davidson_solve_dev": (_i, [_vp, _vp, _vp, _i, C.POINTER(DavidsonOpts),
                                     C.POINTER(DavidsonStats)]),
     "q3b_hegv": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp]),
+    "q3b_start_apply": (_i, [_vp, _vp, _i]),
+    "q3b_start_project": (_i, [_vp, _vp, _vp]),
+    "q3b_start_rotate": (_i, [_vp, _vp, _i, _vp]),
+    "q3b_starting_subspace": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
+    "q3b_server_create": (_i, [_i, _sz, _i, C.POINTER(_vp)]),
+    "q3b_server_destroy": (_i, [_vp]),
+    "q3b_server_last_error": (C.c_char_p, [_vp]),
+    "q3b_server_submit": (_i, [_vp, C.POINTER(Request), C.POINTER(_i)]),
+    "q3b_server_poll": (_i, [_vp, _i]),
+    "q3b_server_wait": (_i, [_vp, _i, _vp, _vp, C.POINTER(DavidsonStats), C.POINTER(RequestTimes)]),
 }
 
 _lib = None

@@ -25,6 +25,7 @@
 // their K range for a fixed-order split-K reduction.  Every mbarrier wait is
 // bounded; a timeout sets an error word and the block drains and frees TMEM.
 #include <cstdint>
+#include <mutex>
 
 #include "cgemm.cuh"
 
@@ -476,9 +477,11 @@ __device__ int g_tc_error;
 
 int* error_word() {
     static int* addr[64] = {};
+    static std::mutex mu;
     int dev = 0;
     Q3B_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
+    std::lock_guard<std::mutex> lk(mu);
     if (!addr[dev]) {
         void* p = nullptr;
         Q3B_CUDA(cudaGetSymbolAddress(&p, g_tc_error));
@@ -506,12 +509,11 @@ size_t workspace_bytes(int M, int N, int K) {
 void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, const float2* A, long lda,
            const float2* B, long ldb, float2 beta, float2* C, long ldc, const GemmWorkspace& ws) {
     int* err = error_word();
-    static bool attr = false;
-    if (!attr) {
-        Q3B_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-        Q3B_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-        attr = true;
-    }
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaFuncSetAttribute(cgemm_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+        cudaFuncSetAttribute(cgemm_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    });
     int splits = conj_a ? choose_splits(M, N, K) : 1;
     const size_t need = (size_t)splits * M * N * sizeof(float2);
     if (splits > 1 && (ws.ptr == nullptr || ws.bytes < need)) splits = 1;

@@ -71,6 +71,38 @@ void Context::require_ready() const {
     if (!kp.valid) throw Status(Q3B_ERR_STATE, "no prepared k-point: call q3b_prepare_kpoint");
 }
 
+static void factor_line(int n, int& na, int& nb) {
+    static const int small[] = {1, 2, 3, 4, 5, 6, 8, 9, 10, 12, 15, 16};
+    na = nb = -1;
+    for (int a : small)
+        for (int b : small)
+            if (a * b == n && a >= b && (na < 0 || a < na)) {
+                na = a;
+                nb = b;
+            }
+    if (na < 0) {
+        throw Status(Q3B_ERR_INVALID,
+                     "FFT length " + std::to_string(n) +
+                         " is not a product of two factors from {2,3,4,5,6,8,9,10,12,15,16}");
+    }
+}
+
+// Position of element i of a line of length n after the backward transform's
+// passes (fft_core.cuh): element k1 + na*k2 sits at nb*k1 + k2.  The identity
+// for a length with no supported factorisation, which the plan build rejects.
+static std::vector<int> transformed_positions(int n) {
+    std::vector<int> pos(n);
+    int na = n, nb = 1;
+    try {
+        factor_line(n, na, nb);
+    } catch (const Status&) {
+        na = n;
+        nb = 1;
+    }
+    for (int i = 0; i < n; ++i) pos[i] = nb * (i % na) + i / na;
+    return pos;
+}
+
 void Context::set_potential(const double* v, int a, int b, int c) {
     if (a <= 0 || b <= 0 || c <= 0 || !v) throw Status(Q3B_ERR_INVALID, "bad potential grid");
     const bool regrid = (a != n1 || b != n2 || c != n3);
@@ -82,11 +114,12 @@ void Context::set_potential(const double* v, int a, int b, int c) {
     std::vector<double> vp(N);
     std::vector<float> vp32(N);
     const double inv = 1.0 / static_cast<double>(N);
+    const std::vector<int> pos2 = transformed_positions(b), pos3 = transformed_positions(c);
     for (int w1 = 0; w1 < a; ++w1)
         for (int w2 = 0; w2 < b; ++w2)
             for (int w3 = 0; w3 < c; ++w3) {
                 const double s = v[((size_t)w1 * b + w2) * c + w3] * inv;
-                const size_t d = ((size_t)w3 * a + w1) * b + w2;
+                const size_t d = ((size_t)pos3[w3] * a + w1) * b + pos2[w2];
                 vp[d] = s;
                 vp32[d] = static_cast<float>(s);
             }
@@ -104,22 +137,6 @@ void Context::set_potential(const double* v, int a, int b, int c) {
     }
     kp.lp64.vplane = v64.as<double>();
     kp.lp32.vplane = v32.as<float>();
-}
-
-static void factor_line(int n, int& na, int& nb) {
-    static const int small[] = {1, 2, 3, 4, 5, 6, 8, 9, 10, 12, 15, 16};
-    na = nb = -1;
-    for (int a : small)
-        for (int b : small)
-            if (a * b == n && a >= b && (na < 0 || a < na)) {
-                na = a;
-                nb = b;
-            }
-    if (na < 0) {
-        throw Status(Q3B_ERR_INVALID,
-                     "FFT length " + std::to_string(n) +
-                         " is not a product of two factors from {2,3,4,5,6,8,9,10,12,15,16}");
-    }
 }
 
 template <typename T, typename R> static std::vector<T> twiddles(int n) {
@@ -218,7 +235,7 @@ void Context::build_plan() {
         lp.na3 = f[4];
         lp.nb3 = f[5];
         lp.sg = 32;
-        lp.plane_items = std::is_same<std::remove_const_t<RR>, double>::value ? 1 : 2;
+        lp.plane_threads = 256;
         lp.nunmapped = static_cast<int>(unm.size());
         lp.stick_start = k.stick_start.as<int>();
         lp.entry_g = k.entry_g.as<int>();
@@ -329,15 +346,14 @@ template <typename R> void Context::tune_local() {
     Q3B_CUDA(cudaMemsetAsync(tin, 0, n * sizeof(T), stream));
     const int chunk = sticks_chunk<R>(nb);
     ws_sticks.reserve(this, (size_t)chunk * sticks_bytes_per_band(lp));
-    const int cand[3] = {1, 2, 4};
-    const int ncand = std::is_same<R, double>::value ? 2 : 3;
+    const int cand[3] = {128, 256, 512};
     cudaEvent_t e0, e1;
     Q3B_CUDA(cudaEventCreate(&e0));
     Q3B_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
-    int best_items = lp.plane_items;
-    for (int c = 0; c < ncand; ++c) {
-        lp.plane_items = cand[c];
+    int best_threads = lp.plane_threads;
+    for (int c = 0; c < 3; ++c) {
+        lp.plane_threads = cand[c];
         float t = 1e30f;
         for (int rep = 0; rep < 3; ++rep) {
             Q3B_CUDA(cudaEventRecord(e0, stream));
@@ -350,10 +366,10 @@ template <typename R> void Context::tune_local() {
         }
         if (t < best) {
             best = t;
-            best_items = cand[c];
+            best_threads = cand[c];
         }
     }
-    lp.plane_items = best_items;
+    lp.plane_threads = best_threads;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     ws_tune.release();

@@ -67,13 +67,17 @@ class Context {
     int n1 = 0, n2 = 0, n3 = 0;
     bool pot_valid = false;
     std::vector<double> v_host;     // V(r) as given, reference layout
-    DevBuf v64, v32;                // V/N, [w3][w1][w2]
+    DevBuf v64, v32;                // V/N, [w3 pos][w1][w2 pos] (see LocalPlan::vplane)
 
     KPoint kp;
 
     // workspaces
     DevBuf ws_sticks, ws_gemm, ws_bm, ws_bp, ws_conv_in, ws_conv_out, ws_host_io;
     DevBuf ws_solver, ws_dense, ws_bands, ws_tune;
+    // starting-subspace rotation: chi and H chi of the last q3b_start_apply
+    DevBuf ws_start;
+    int start_n = 0;
+    int start_npw = 0;
 
     explicit Context(int dev, size_t hbm_budget);
     ~Context();

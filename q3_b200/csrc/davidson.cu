@@ -608,6 +608,8 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         s.unconverged = r.unconverged;
         s.collapses = r.collapses;
         s.max_residual_norm = r.resid;
+        Q3B_CUDA(cudaStreamSynchronize(c.stream));
+        s.fp64_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     } else if (o.precision == Q3B_MIXED) {
         // FP32 phase to the loose tolerance
         std::vector<double> eig32;
@@ -626,6 +628,7 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
             col32 = r.collapses;
         }
         // FP64 refinement sweeps from the FP32 Ritz pairs
+        const auto t64 = std::chrono::steady_clock::now();
         Davidson<double> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
         Q3B_CUDA(cudaMemcpyAsync(dv.V(), bands_dev, band_bytes, cudaMemcpyDeviceToDevice, c.stream));
         const int sweeps = o.refine_sweeps > 0 ? o.refine_sweeps : 6;
@@ -638,6 +641,8 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         s.unconverged = r.unconverged;
         s.collapses = col32 + r.collapses;
         s.max_residual_norm = r.resid;
+        Q3B_CUDA(cudaStreamSynchronize(c.stream));
+        s.fp64_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t64).count();
     } else {
         throw Status(Q3B_ERR_INVALID, "unknown precision");
     }

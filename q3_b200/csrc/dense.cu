@@ -16,6 +16,7 @@
 //         then the reflectors applied back (one warp per vector).
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "context.cuh"
@@ -30,57 +31,72 @@ constexpr int NB = 32;
 
 __device__ __forceinline__ int vload(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
 
+__device__ __forceinline__ double2 warp_sum(double2 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // ------------------------------------------------------------------ potrf
-// Diagonal block k: one warp factors the 32x32 block (lane c owns column c)
-// and inverts the triangular factor (lane c computes column c of U^-1).
-__global__ void __launch_bounds__(32)
+// Diagonal block k, 32x32 threads: warp c, lane r owns element (r, c).  At
+// step j every (r, c) with j < r <= c subtracts conj(G(j,r)) G(j,c) / G(j,j)
+// (row j of U times its conjugate, taken from the unscaled row) while row j
+// is scaled into U: one barrier a step.  Then U^{-1} a column per warp: lane t
+// holds X(t, c) and row r, from the bottom up, is a warp sum.
+__global__ void __launch_bounds__(1024)
 potrf_diag(int n, int k, double2* A, int lda, double2* dinv, int* info) {
     if (vload(info)) return;
-    __shared__ double2 a[NB][NB + 1];  // a[c][r] = element (r, c)
-    __shared__ double2 x[NB][NB + 1];
+    __shared__ double2 a[NB][NB + 1];  // a[c][r] = G(r, c)
+    __shared__ double2 u[NB][NB + 1];  // u[c][r] = U(r, c)
+    const int r = threadIdx.x & 31, c = threadIdx.x >> 5;
     const int r0 = k * NB;
     const int bs = min(NB, n - r0);
-    const int c = threadIdx.x;
-    for (int r = 0; r < NB; ++r) {
+    {
         double2 v = (r == c) ? mk(1.0, 0.0) : mk(0.0, 0.0);
-        if (r < bs && c < bs) v = A[(r0 + r) + (long)(r0 + c) * lda];
+        if (r < bs && c < bs && r <= c) v = A[(r0 + r) + (long)(r0 + c) * lda];
         a[c][r] = v;
-        x[c][r] = mk(0.0, 0.0);
+        u[c][r] = mk(0.0, 0.0);
     }
-    __syncwarp();
+    __syncthreads();
     int bad = 0;
     for (int j = 0; j < NB; ++j) {
-        // lane j takes the pivot; every lane reads it
         double piv = a[j][j].x;
         if (!(piv > 0.0)) {
             if (!bad && j < bs) bad = r0 + j + 1;
             piv = 1.0;
         }
-        const double u = sqrt(piv);
-        __syncwarp();
-        if (c == j) a[j][j] = mk(u, 0.0);
-        if (c > j) a[c][j] = mk(a[c][j].x / u, a[c][j].y / u);   // U(j, c)
-        __syncwarp();
-        // trailing update of column c: G(r, c) -= conj(U(j, r)) U(j, c), j < r <= c
-        if (c > j) {
-            const double2 ujc = a[c][j];
-            for (int r = j + 1; r <= c; ++r) a[c][r] = a[c][r] - cmulc(a[r][j], ujc);
+        if (r == j && c >= j) {
+            const double us = sqrt(piv);
+            u[c][j] = (c == j) ? mk(us, 0.0) : mk(a[c][j].x / us, a[c][j].y / us);
         }
-        __syncwarp();
+        if (j < r && r <= c) {
+            const double2 g = cmulc(a[r][j], a[c][j]);  // conj(G(j,r)) G(j,c)
+            a[c][r] = a[c][r] - mk(g.x / piv, g.y / piv);
+        }
+        __syncthreads();
     }
-    // X = U^{-1}, column c by lane c
-    for (int r = c; r >= 0; --r) {
-        double2 s = (r == c) ? mk(1.0, 0.0) : mk(0.0, 0.0);
-        for (int t = r + 1; t <= c; ++t) s = s - cmul(a[t][r], x[c][t]);
-        const double u = a[r][r].x;
-        x[c][r] = mk(s.x / u, s.y / u);
+    // column c of X = U^{-1}; lane t holds X(t, c)
+    double2 x = mk(0.0, 0.0);
+    for (int rr = c; rr >= 0; --rr) {
+        double2 p = (rr < r && r <= c) ? cmul(u[r][rr], x) : mk(0.0, 0.0);
+        p = warp_sum(p);
+        if (r == rr) {
+            const double2 rhs = (rr == c) ? mk(1.0 - p.x, -p.y) : mk(-p.x, -p.y);
+            const double ud = u[rr][rr].x;
+            x = mk(rhs.x / ud, rhs.y / ud);
+        }
     }
-    __syncwarp();
-    for (int r = 0; r < NB; ++r) {
-        if (r < bs && c < bs && r <= c) A[(r0 + r) + (long)(r0 + c) * lda] = a[c][r];
-        dinv[(long)k * NB * NB + r + c * NB] = x[c][r];
-    }
-    if (c == 0 && bad) atomicCAS(info, 0, bad);
+    if (r < bs && c < bs && r <= c) A[(r0 + r) + (long)(r0 + c) * lda] = u[c][r];
+    dinv[(long)k * NB * NB + r + c * NB] = x;
+    if (threadIdx.x == 0 && bad) atomicCAS(info, 0, bad);
 }
 
 // U(k, j) = U_kk^{-H} G(k, j) for every block column j > k
@@ -263,18 +279,20 @@ __device__ __forceinline__ bool grid_sync(unsigned* bar, unsigned nblocks, int* 
     return s_ok != 0;
 }
 
-__device__ __forceinline__ double2 warp_sum(double2 v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+// one thread waits (bounded) for a flag raised with st.release; false when it
+// gave up or another block reported an error
+__device__ __forceinline__ bool wait_flag(const unsigned* flag, int* err) {
+    const long long t0 = clock64();
+    while (true) {
+        unsigned f;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(f) : "l"(flag) : "memory");
+        if (f != 0u) return true;
+        if (vload(err)) return false;
+        if (clock64() - t0 > (1LL << 32)) {
+            atomicExch(err, 1);
+            return false;
+        }
     }
-    return v;
-}
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
 }
 
 // ------------------------------------------------------------------ hetrd
@@ -284,14 +302,18 @@ __device__ __forceinline__ double warp_sum(double v) {
 // so that A = Q T Q^H and an eigenvector of A is W^H times one of T.
 // Block b owns columns c = b + G*j (cyclic, G = gridDim.x); it keeps them in
 // shared memory for the whole reduction, and its columns of W too when they
-// fit (`w_in_smem`), else in global memory.  Per column step, two grid
-// barriers: one after every block has published its entries of p = tau A v
-// and its share of v^H p, one after the owner of column k+1 has updated and
-// published it.  Only that column, p and the shares cross blocks, through L2
-// (ld.global.cg); every wait is bounded.
-__global__ void __launch_bounds__(256)
+// fit (`w_in_smem`), else in global memory.  Per column step, one grid
+// barrier, after every block has published its entries of p = tau A v and its
+// share of v^H p; and one flag, set by the owner of column k+1 once it has
+// updated and published that column, which the other blocks wait for before
+// the next step.  p and the shares are double-buffered by step parity: a
+// block can run at most one step ahead of another (the barrier of the next
+// step holds it), so it never overwrites values still being read.  Only
+// column k+1, p and the shares cross blocks, through L2 (ld.global.cg);
+// every wait is bounded.
+__global__ void __launch_bounds__(256, 1)
 hetrd_smem(int n, int cpb, int w_in_smem, const double2* A, double* d, double2* e, double2* W,
-           double2* xbuf, double2* pbuf, double2* partial, unsigned* bar, int* err) {
+           double2* xbuf, double2* pbuf2, double2* partial2, unsigned* bar, unsigned* ready, int* err) {
     extern __shared__ __align__(16) unsigned char smem[];
     double2* cols = reinterpret_cast<double2*>(smem);   // cpb columns of A
     double2* sv = cols + (size_t)cpb * n;              // v
@@ -316,8 +338,17 @@ hetrd_smem(int n, int cpb, int w_in_smem, const double2* A, double* d, double2* 
     if (b == 0)
         for (int r = tid; r < n; r += blockDim.x) xbuf[r] = A[r];
     if (!grid_sync(bar, G, err)) return;
+    __shared__ int s_go;
     for (int k = 0; k + 1 < n; ++k) {
         const int m = n - k - 1;
+        double2* pbuf = pbuf2 + (size_t)(k & 1) * n;
+        double2* partial = partial2 + (size_t)(k & 1) * G;
+        // column k, rows k+1.., as published by its owner (step k-1)
+        if (k > 0 && k % G != b) {
+            if (tid == 0) s_go = wait_flag(ready + k, err);
+            __syncthreads();
+            if (!s_go) return;
+        }
         double part = 0.0;
         for (int j = tid; j < m; j += blockDim.x) {
             const double2 x = __ldcg(&xbuf[k + 1 + j]);
@@ -373,10 +404,11 @@ hetrd_smem(int n, int cpb, int w_in_smem, const double2* A, double* d, double2* 
         }
         if (!grid_sync(bar, G, err)) return;
         if (tk != 0.0) {
-            if (tid == 0) {
+            if (warp == 0) {
                 double2 sacc = mk(0.0, 0.0);
-                for (int q = 0; q < G; ++q) sacc = sacc + __ldcg(&partial[q]);
-                redc[0] = sacc;
+                for (int q = lane; q < G; q += 32) sacc = sacc + __ldcg(&partial[q]);
+                sacc = warp_sum(sacc);
+                if (lane == 0) redc[0] = sacc;
             }
             __syncthreads();
             const double half = 0.5 * tk * redc[0].x;  // v^H p is real
@@ -406,14 +438,17 @@ hetrd_smem(int n, int cpb, int w_in_smem, const double2* A, double* d, double2* 
         }
         __syncthreads();
         // the owner of column k+1 publishes its rows k+1.. for the next step
+        // and raises its flag; it reads the column from its own shared memory
         if ((k + 1) % G == b) {
             const double2* col = cols + (size_t)((k + 1) / G) * n;
             for (int r = k + 1 + tid; r < n; r += blockDim.x) xbuf[r] = col[r];
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ready + k + 1), "r"(1u) : "memory");
         }
-        if (!grid_sync(bar, G, err)) return;
     }
     if (b == 0 && tid == 0) {
-        d[n - 1] = __ldcg(&xbuf[n - 1]).x;
+        if (n < 2 || (n - 1) % G == 0 || wait_flag(ready + n - 1, err)) d[n - 1] = __ldcg(&xbuf[n - 1]).x;
         e[n - 1] = mk(0.0, 0.0);
     }
     if (w_in_smem) {
@@ -492,37 +527,58 @@ __global__ void apply_phase(int n, int nvec, const double2* phase, const double*
     }
 }
 
-// number of eigenvalues of the real tridiagonal (d, e2) below x
-__device__ __forceinline__ int sturm_count(int n, const double* d, const double* e2, double x, double pivmin) {
-    int c = 0;
-    double q = d[0] - x;
-    if (fabs(q) < pivmin) q = -pivmin;
-    c += q < 0.0;
-    for (int k = 1; k < n; ++k) {
-        q = (d[k] - x) - e2[k - 1] / q;
-        if (fabs(q) < pivmin) q = -pivmin;
-        c += q < 0.0;
+// numbers of eigenvalues of the real tridiagonal (d, e2) below x[0..S): S
+// independent recurrences interleaved, so their divisions overlap
+template <int S>
+__device__ __forceinline__ void sturm_counts(int n, const double* d, const double* e2, const double* x,
+                                             double pivmin, int* c) {
+    double q[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        q[s] = d[0] - x[s];
+        if (fabs(q[s]) < pivmin) q[s] = -pivmin;
+        c[s] = q[s] < 0.0;
     }
-    return c;
+    for (int k = 1; k < n; ++k) {
+        const double dk = d[k], ek = e2[k - 1];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            q[s] = (dk - x[s]) - ek / q[s];
+            if (fabs(q[s]) < pivmin) q[s] = -pivmin;
+            c[s] += q[s] < 0.0;
+        }
+    }
 }
 
-// one warp per eigenvalue: 32-point multisection of [lo, hi] on Sturm counts
+// one warp per eigenvalue: multisection of [lo, hi] on Sturm counts at
+// 32 x kShifts interior points per round (the interval shrinks 129-fold)
+constexpr int kShifts = 4;
 __global__ void tridiag_multisect(int n, const double* d, const double* e2, const double* bounds, double* w) {
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= n) return;
+    constexpr int P = 32 * kShifts;  // points per round
     double a = bounds[0], b = bounds[1];
     const double scale = bounds[2];
     const double pivmin = fmax(1e-290, 1e-300 * scale * scale);
     const double tol = 4.0 * 2.220446049250313e-16 * fmax(scale, 1e-300);
     for (int it = 0; it < 64 && (b - a) > tol; ++it) {
-        const double x = a + (b - a) * (lane + 1) / 33.0;
-        const int cnt = sturm_count(n, d, e2, x, pivmin);
-        // first lane whose point has more than i eigenvalues below it
-        const unsigned above = __ballot_sync(0xffffffffu, cnt > i);
+        double x[kShifts];
+        int cnt[kShifts];
+#pragma unroll
+        for (int s = 0; s < kShifts; ++s) x[s] = a + (b - a) * (lane * kShifts + s + 1) / (P + 1.0);
+        sturm_counts<kShifts>(n, d, e2, x, pivmin, cnt);
+        // first point (in order lane*kShifts + s) with more than i eigenvalues below it
+        int first = kShifts;
+#pragma unroll
+        for (int s = kShifts - 1; s >= 0; --s)
+            if (cnt[s] > i) first = s;
+        const unsigned above = __ballot_sync(0xffffffffu, first < kShifts);
         const int l = above ? __ffs(above) - 1 : 32;
-        const double na = (l == 0) ? a : a + (b - a) * l / 33.0;
-        const double nb = (l == 32) ? b : a + (b - a) * (l + 1) / 33.0;
+        const int fl = __shfl_sync(0xffffffffu, first, l & 31);
+        const int m = (l == 32) ? P : l * kShifts + fl;
+        const double na = (m == 0) ? a : a + (b - a) * m / (P + 1.0);
+        const double nb = (m == P) ? b : a + (b - a) * (m + 1) / (P + 1.0);
         a = na;
         b = nb;
     }
@@ -615,6 +671,116 @@ __global__ void tridiag_invit(int n, const double* d, const double* ea, const do
     }
 }
 
+// The same inverse iteration with each thread's factors and iterate in shared
+// memory, laid out [t][thread] (a warp's accesses fall in distinct banks), the
+// recurrences carried in registers and the pivots' reciprocals stored, so a
+// step of each sweep is a few shared-memory accesses and fused multiply-adds.
+// blockDim.x threads (one per eigenvalue) share the block's shared memory:
+// 41 bytes per thread and row.
+__device__ __forceinline__ double clamp_tiny(double x, double tiny) {
+    return fabs(x) < tiny ? (x < 0.0 ? -tiny : tiny) : x;
+}
+
+__global__ void tridiag_invit_smem(int n, const double* d, const double* ea, const double* w,
+                                   const double* bounds, int nvec, double* Y) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = blockDim.x, tid = threadIdx.x;
+    double* DL = reinterpret_cast<double*>(smem);
+    double* DU = DL + (size_t)n * T;
+    double* DU2 = DU + (size_t)n * T;
+    double* DI = DU2 + (size_t)n * T;
+    double* y = DI + (size_t)n * T;
+    unsigned char* piv = reinterpret_cast<unsigned char*>(y + (size_t)n * T);
+    const int i = blockIdx.x * T + tid;
+    if (i >= nvec) return;
+    const double scale = fmax(bounds[2], 1e-300);
+    const double ortol = 1e-5 * scale;
+    if (i > 0 && w[i] - w[i - 1] <= ortol) return;
+    int jend = i + 1;
+    while (jend < nvec && w[jend] - w[jend - 1] <= ortol) ++jend;
+    const double eps = 2.220446049250313e-16;
+    const double tiny = eps * scale;
+    double lam_prev = 0.0;
+#define AT(t) ((size_t)(t) * T + tid)
+    for (int j = i; j < jend; ++j) {
+        double lam = w[j];
+        if (j > i && lam - lam_prev < 10.0 * eps * scale) lam = lam_prev + 10.0 * eps * scale;
+        lam_prev = lam;
+        // LU with partial pivoting of T - lam I; (dcur, ducur) = row t's
+        // diagonal and superdiagonal as modified by the steps before it
+        double dcur = d[0] - lam, ducur = n > 1 ? ea[0] : 0.0;
+        for (int t = 0; t + 1 < n; ++t) {
+            const double sub = ea[t];
+            const double dnext = d[t + 1] - lam;
+            const double dunext = (t + 2 < n) ? ea[t + 1] : 0.0;
+            if (fabs(dcur) >= fabs(sub)) {
+                if (dcur == 0.0) dcur = tiny;
+                const double f = sub / dcur;
+                DL[AT(t)] = f;
+                DU[AT(t)] = ducur;
+                DU2[AT(t)] = 0.0;
+                DI[AT(t)] = 1.0 / clamp_tiny(dcur, tiny);
+                piv[AT(t)] = 0;
+                dcur = dnext - f * ducur;
+                ducur = dunext;
+            } else {
+                const double f = dcur / sub;
+                DL[AT(t)] = f;
+                DU[AT(t)] = dnext;
+                DU2[AT(t)] = dunext;
+                DI[AT(t)] = 1.0 / clamp_tiny(sub, tiny);
+                piv[AT(t)] = 1;
+                dcur = ducur - f * dnext;
+                ducur = -f * dunext;
+            }
+        }
+        DI[AT(n - 1)] = 1.0 / clamp_tiny(dcur, tiny);
+        for (int t = 0; t < n; ++t) y[AT(t)] = 1.0 + 0.25 * sin(0.7 * t + 1.3 * j);
+        double ys = 1.0;  // pending normalisation of y
+        for (int iter = 0; iter < 3; ++iter) {
+            double ycur = y[AT(0)] * ys;
+            for (int t = 0; t + 1 < n; ++t) {
+                const double ynext = y[AT(t + 1)] * ys;
+                const double f = DL[AT(t)];
+                if (!piv[AT(t)]) {
+                    y[AT(t)] = ycur;
+                    ycur = ynext - f * ycur;
+                } else {
+                    y[AT(t)] = ynext;
+                    ycur = ycur - f * ynext;
+                }
+            }
+            double y1 = ycur * DI[AT(n - 1)], y2 = 0.0;
+            y[AT(n - 1)] = y1;
+            double nr = y1 * y1;
+            for (int t = n - 2; t >= 0; --t) {
+                const double v = (y[AT(t)] - DU[AT(t)] * y1 - DU2[AT(t)] * y2) * DI[AT(t)];
+                y[AT(t)] = v;
+                nr += v * v;
+                y2 = y1;
+                y1 = v;
+            }
+            if (j > i) {
+                for (int q = i; q < j; ++q) {
+                    const double* yq = Y + (size_t)q * n;
+                    double s = 0.0;
+                    for (int t = 0; t < n; ++t) s += yq[t] * y[AT(t)];
+                    for (int t = 0; t < n; ++t) y[AT(t)] -= s * yq[t];
+                }
+                nr = 0.0;
+                for (int t = 0; t < n; ++t) nr += y[AT(t)] * y[AT(t)];
+            }
+            ys = 1.0 / sqrt(nr);
+        }
+        double* yo = Y + (size_t)j * n;
+        for (int t = 0; t < n; ++t) yo[t] = y[AT(t)] * ys;
+    }
+#undef AT
+}
+
+constexpr size_t kInvitSmemLimit = 200 * 1024;
+constexpr int kInvitBytesPerRow = 5 * sizeof(double) + 1;
+
 struct Chol {
     double2* dinv;
     int* info;
@@ -632,7 +798,7 @@ int potrf_impl(cudaStream_t st, int n, double2* A, int lda, const Chol& c) {
     const int nblk = ceil_div(n, NB);
     Q3B_CUDA(cudaMemsetAsync(c.info, 0, sizeof(int), st));
     for (int k = 0; k < nblk; ++k) {
-        potrf_diag<<<1, 32, 0, st>>>(n, k, A, lda, c.dinv, c.info);
+        potrf_diag<<<1, 1024, 0, st>>>(n, k, A, lda, c.dinv, c.info);
         Q3B_LAUNCH_CHECK();
         const int m = nblk - k - 1;
         if (m > 0) {
@@ -672,7 +838,8 @@ size_t hegv_scratch_bytes(int n) {
     // eigenvector; a few length-n vectors; 256-byte alignment slack
     const size_t nn = (size_t)n * n;
     return potrf_scratch_bytes(n) + 5 * nn * sizeof(double2) + nn * (sizeof(double2) + 6 * sizeof(double)) +
-           nn * sizeof(double2) + 64 * (size_t)n * sizeof(double2) + 64 * 1024;
+           nn * sizeof(double2) + 64 * (size_t)n * sizeof(double2) + 2 * 148 * sizeof(double2) +
+           (size_t)n * sizeof(unsigned) + 64 * 1024;
 }
 
 int potrf(cudaStream_t st, int n, double2* A, int lda, Scratch& ws) {
@@ -693,7 +860,7 @@ void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, S
     double2* e = ws.take<double2>(n);
     double2* W = ws.take<double2>((size_t)n * n);
     double2* xbuf = ws.take<double2>(n);
-    double2* pbuf = ws.take<double2>(n);
+    double2* pbuf = ws.take<double2>(2 * (size_t)n);
     double* ea = ws.take<double>(n);
     double* e2 = ws.take<double>(n);
     double2* phase = ws.take<double2>(n);
@@ -713,21 +880,21 @@ void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, S
     if (smem > limit) throw Status(Q3B_ERR_INVALID, "subspace of order " + std::to_string(n) + " too large for the eigensolver");
     int w_in_smem = (smem + (size_t)cpb * n * sizeof(double2) <= limit) ? 1 : 0;
     if (w_in_smem) smem += (size_t)cpb * n * sizeof(double2);
-    double2* partial = ws.take<double2>(G);
-    unsigned* bar = ws.take<unsigned>(2);
+    double2* partial = ws.take<double2>(2 * (size_t)G);
+    unsigned* bar = ws.take<unsigned>(2 + (size_t)n);
+    unsigned* ready = bar + 2;
     int* err = ws.take<int>(1);
-    Q3B_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
+    Q3B_CUDA(cudaMemsetAsync(bar, 0, (2 + (size_t)n) * sizeof(unsigned), st));
     Q3B_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
-    static bool attr_set = false;
-    if (!attr_set) {
-        Q3B_CUDA(cudaFuncSetAttribute(hetrd_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit));
-        attr_set = true;
-    }
+    static std::once_flag once;
+    std::call_once(once, [limit] {
+        cudaFuncSetAttribute(hetrd_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit);
+    });
     int per_sm = 0;
     Q3B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_smem, 256, smem));
     if (per_sm < 1 || per_sm * nsm < G) throw Status(Q3B_ERR_INVALID, "eigensolver blocks cannot be co-resident");
     const double2* Ac = A;
-    void* args[] = {&n, &cpb, &w_in_smem, &Ac, &d, &e, &W, &xbuf, &pbuf, &partial, &bar, &err};
+    void* args[] = {&n, &cpb, &w_in_smem, &Ac, &d, &e, &W, &xbuf, &pbuf, &partial, &bar, &ready, &err};
     Q3B_CUDA(cudaLaunchCooperativeKernel((const void*)hetrd_smem, dim3(G), dim3(256), args, smem, st));
     Q3B_LAUNCH_CHECK();
     tridiag_prep<<<1, 32, 0, st>>>(n, d, e, ea, e2, phase, bounds);
@@ -735,7 +902,18 @@ void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, S
     tridiag_multisect<<<ceil_div((long)n * 32, 256), 256, 0, st>>>(n, d, e2, bounds, w);
     Q3B_LAUNCH_CHECK();
     if (nvec > 0) {
-        tridiag_invit<<<ceil_div(nvec, 64), 64, 0, st>>>(n, d, ea, w, bounds, nvec, Y, work);
+        const int T = static_cast<int>(std::min<size_t>(64, kInvitSmemLimit / ((size_t)n * kInvitBytesPerRow)));
+        if (T >= 1) {
+            static std::once_flag once_inv;
+            std::call_once(once_inv, [] {
+                cudaFuncSetAttribute(tridiag_invit_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kInvitSmemLimit);
+            });
+            const size_t sm = (size_t)n * T * kInvitBytesPerRow;
+            tridiag_invit_smem<<<ceil_div(nvec, T), T, sm, st>>>(n, d, ea, w, bounds, nvec, Y);
+        } else {
+            tridiag_invit<<<ceil_div(nvec, 64), 64, 0, st>>>(n, d, ea, w, bounds, nvec, Y, work);
+        }
         Q3B_LAUNCH_CHECK();
         apply_phase<<<grid_for((long)n * nvec), 256, 0, st>>>(n, nvec, phase, Y, Yc);
         Q3B_LAUNCH_CHECK();

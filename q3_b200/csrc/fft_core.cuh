@@ -5,15 +5,10 @@
 //   DIR = -1 : forward,  X_k = sum_j x_j exp(-2 pi i jk/n)
 //   DIR = +1 : backward, X_k = sum_j x_j exp(+2 pi i jk/n)      (both unnormalised)
 //
-// A line of length n = NA * NB is transformed by threads in two steps
-// (Cooley-Tukey with j = n2 + NB*n1, k = k1 + NA*k2):
-//   step 1: item (line, n2): DFT_NA over x[n2 + NB*n1], times w_n^{n2*k1},
-//           written back in place to x[n2 + NB*k1];
-//   step 2: item (line, k1): DFT_NB over x[n2 + NB*k1], written to x[k1 + NA*k2].
-// Step 2 writes where other items read, so every item of step 2 is loaded into
-// registers before a barrier and stored after it.  Lines are spread across
-// lanes (line index fastest) so that shared-memory accesses of a warp fall on
-// consecutive lines, which the callers lay out at an odd pitch.
+// A line of length n = na * nb is transformed by the threads of a block in
+// two in-place passes (Cooley-Tukey); the backward transform leaves the line
+// in a digit-reversed order that the forward transform takes as its input, so
+// neither needs a reordering pass (see "The line transforms as passes").
 //
 // The twiddle table holds w_n^m = exp(-2 pi i m / n), m < n, in shared memory;
 // the backward direction uses its conjugate.
@@ -147,129 +142,168 @@ struct LineGeom {
     __device__ __forceinline__ int base(int l) const { return bases ? bases[l] : l * ls; }
 };
 
-struct NoEpilogue {
-    template <typename T> __device__ __forceinline__ T operator()(int, int, T v) const { return v; }
-};
+// Position -> index map of the digit-reversed order the backward transform
+// leaves a line in: position nb*k1 + k2 holds element k1 + na*k2.
+__device__ __forceinline__ int digit_reversed(int pos, int na, int nb) { return pos / nb + na * (pos % nb); }
 
-// step 1: in place, no hazard between items.  Item it = l + lines*n2; the
-// (l, n2) pair is stepped by blockDim without dividing in the loop.
-template <int NA, int DIR, typename T>
-__device__ __forceinline__ void line_step1(T* buf, const LineGeom& g, const T* tw) {
-    const int items = g.lines * g.nb;
-    const int tws = g.n / NA;
+// One in-place pass over every line.  Item (l, q) owns the R values of line l
+// at positions q*qs + r*rs, r < R:
+//   CONTIG = false: q < nb, positions q + nb*r      (R = na, stride nb)
+//   CONTIG = true : q < na, positions nb*q + r      (R = nb, contiguous)
+// Either way the items of a line partition it, so a pass is one read and one
+// write of every element with no hazard between items, and passes are
+// separated by one barrier.  Lines run fastest across lanes: the callers lay
+// lines out at an odd pitch, so a warp's accesses fall in distinct banks.
+template <int R, bool CONTIG, typename T, typename Body>
+__device__ __forceinline__ void line_pass(T* buf, const LineGeom& g, const Body& body) {
+    const int Q = CONTIG ? g.na : g.nb;
+    const int qs = (CONTIG ? g.nb : 1) * g.es;
+    const int rs = (CONTIG ? 1 : g.nb) * g.es;
+    const int items = g.lines * Q;
     const int bq = static_cast<int>(blockDim.x) / g.lines, br = static_cast<int>(blockDim.x) % g.lines;
-    int l = static_cast<int>(threadIdx.x) % g.lines, n2 = static_cast<int>(threadIdx.x) / g.lines;
+    int l = static_cast<int>(threadIdx.x) % g.lines, q = static_cast<int>(threadIdx.x) / g.lines;
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        T* p = buf + g.base(l) + n2 * g.es;
-        T x[NA];
+        T* p = buf + g.base(l) + q * qs;
+        T x[R];
 #pragma unroll
-        for (int n1 = 0; n1 < NA; ++n1) x[n1] = p[n1 * g.nb * g.es];
-        dft<NA, DIR>(x, tw, tws);
+        for (int r = 0; r < R; ++r) x[r] = p[r * rs];
+        body(x, l, q);
 #pragma unroll
-        for (int k1 = 0; k1 < NA; ++k1) {
-            const int m = n2 * k1;  // < n
-            T v = (k1 == 0 || n2 == 0) ? x[k1] : cmul(x[k1], twiddle<DIR>(tw, m));
-            p[k1 * g.nb * g.es] = v;
-        }
+        for (int r = 0; r < R; ++r) p[r * rs] = x[r];
         l += br;
-        n2 += bq;
+        q += bq;
         if (l >= g.lines) {
             l -= g.lines;
-            ++n2;
+            ++q;
         }
     }
 }
 
-// step 2: an item's stores land in other items' inputs, but only within its
-// own line.  Lines are therefore taken in rounds of whole lines: every item of
-// a round is loaded into registers before a barrier and stored after it.
-// MAXIT bounds the items one thread holds per round.
-template <int NB, int DIR, int MAXIT, typename T, typename Epi>
-__device__ __forceinline__ void line_step2(T* buf, const LineGeom& g, const T* tw, const Epi& epi) {
+// The line transforms as passes (Cooley-Tukey, n = na*nb, DIR +1 backward,
+// -1 forward, both unnormalised):
+//   backward, natural order in, digit-reversed order out:
+//     A+ : DFT_na over x[n2 + nb*n1] (n1 < na) for each n2 < nb, times
+//          w^{+n2*k1}, in place;
+//     B+ : DFT_nb over the contiguous block nb*k1 + n2 (n2 < nb) for each
+//          k1 < na, in place: position nb*k1 + k2 now holds X[k1 + na*k2].
+//   forward, digit-reversed order in, natural order out (the factorisation
+//   with the roles of na and nb swapped, j = n2 + na*n1, k = k1 + nb*k2):
+//     B- : DFT_nb over the contiguous block nb*n2 + n1 (n1 < nb), the
+//          elements y[n2 + na*n1], times w^{-n2*k1}, in place;
+//     A- : DFT_na over positions nb*n2 + k1 (n2 < na) for each k1 < nb,
+//          in place: position k1 + nb*k2 now holds Y[k1 + nb*k2].
+// A backward-then-forward round trip fuses B+ and B- in registers, with an
+// epilogue applied to each value at its natural index between them.
+
+template <int NA, int DIR, typename T>
+__device__ __forceinline__ void pass_a(T* buf, const LineGeom& g, const T* tw) {
+    const int tws = g.n / NA;
+    line_pass<NA, false>(buf, g, [&](T* x, int, int q) {
+        dft<NA, DIR>(x, tw, tws);
+        if (DIR > 0) {
+#pragma unroll
+            for (int k = 1; k < NA; ++k)
+                if (q != 0) x[k] = cmul(x[k], twiddle<DIR>(tw, q * k));  // q*k < n
+        }
+    });
+}
+
+template <int NB, int DIR, typename T>
+__device__ __forceinline__ void pass_b(T* buf, const LineGeom& g, const T* tw) {
     const int tws = g.n / NB;
-    int per_round = (static_cast<int>(blockDim.x) * MAXIT) / g.na;
-    if (per_round < 1) per_round = 1;
-    for (int l0 = 0; l0 < g.lines; l0 += per_round) {
-        const int lr = min(per_round, g.lines - l0);
-        const int items = lr * g.na;
-        const int bq = static_cast<int>(blockDim.x) / lr, br = static_cast<int>(blockDim.x) % lr;
-        const int lt = static_cast<int>(threadIdx.x) % lr, kt = static_cast<int>(threadIdx.x) / lr;
-        T x[MAXIT][NB];
-        int ls[MAXIT], ks[MAXIT];
-        {
-            int l = lt, k1 = kt;
+    line_pass<NB, true>(buf, g, [&](T* x, int, int q) {
+        dft<NB, DIR>(x, tw, tws);
+        if (DIR < 0) {
 #pragma unroll
-            for (int r = 0; r < MAXIT; ++r) {
-                ls[r] = l0 + l;
-                ks[r] = k1;
-                l += br;
-                k1 += bq;
-                if (l >= lr) {
-                    l -= lr;
-                    ++k1;
-                }
-            }
+            for (int k = 1; k < NB; ++k)
+                if (q != 0) x[k] = cmul(x[k], twiddle<DIR>(tw, q * k));  // q*k < n
         }
+    });
+}
+
+template <int NB, typename T, typename Epi>
+__device__ __forceinline__ void pass_mid(T* buf, const LineGeom& g, const T* tw, const Epi& epi) {
+    const int tws = g.n / NB;
+    const int na = g.na;
+    line_pass<NB, true>(buf, g, [&](T* x, int l, int q) {
+        dft<NB, +1>(x, tw, tws);
 #pragma unroll
-        for (int r = 0; r < MAXIT; ++r) {
-            const int it = threadIdx.x + r * blockDim.x;
-            if (it < items) {
-                const T* p = buf + g.base(ls[r]) + ks[r] * g.nb * g.es;
+        for (int r = 0; r < NB; ++r) x[r] = epi(l, q + na * r, x[r]);
+        dft<NB, -1>(x, tw, tws);
 #pragma unroll
-                for (int n2 = 0; n2 < NB; ++n2) x[r][n2] = p[n2 * g.es];
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < MAXIT; ++r) {
-            const int it = threadIdx.x + r * blockDim.x;
-            if (it < items) {
-                const int l = ls[r];
-                const int k1 = ks[r];
-                dft<NB, DIR>(x[r], tw, tws);
-                T* p = buf + g.base(l);
-#pragma unroll
-                for (int k2 = 0; k2 < NB; ++k2) {
-                    const int j = k1 + g.na * k2;
-                    p[j * g.es] = epi(l, j, x[r][k2]);
-                }
-            }
-        }
-        __syncthreads();
-    }
+        for (int k = 1; k < NB; ++k)
+            if (q != 0) x[k] = cmul(x[k], twiddle<-1>(tw, q * k));
+    });
 }
 
 #define Q3B_FFT_SIZES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(8) X(9) X(10) X(12) X(15) X(16)
 
-template <int DIR, typename T>
-__device__ __forceinline__ void run_step1(T* buf, const LineGeom& g, const T* tw) {
+// MAXR: the largest factor a caller instantiates (lengths with a larger
+// factor are not transformed); a smaller bound keeps registers down.
+template <int DIR, int MAXR, typename T>
+__device__ __forceinline__ void run_a(T* buf, const LineGeom& g, const T* tw) {
     switch (g.na) {
-#define Q3B_S1(N) \
-    case N: line_step1<N, DIR>(buf, g, tw); break;
-        Q3B_FFT_SIZES(Q3B_S1)
-#undef Q3B_S1
+#define Q3B_A(N) \
+    case N:                                                 \
+        if constexpr (N <= MAXR) pass_a<N, DIR>(buf, g, tw); \
+        break;
+        Q3B_FFT_SIZES(Q3B_A)
+#undef Q3B_A
         default: break;
     }
 }
 
-template <int DIR, int MAXIT, typename T, typename Epi>
-__device__ __forceinline__ void run_step2(T* buf, const LineGeom& g, const T* tw, const Epi& epi) {
+template <int DIR, int MAXR, typename T>
+__device__ __forceinline__ void run_b(T* buf, const LineGeom& g, const T* tw) {
     switch (g.nb) {
-#define Q3B_S2(N) \
-    case N: line_step2<N, DIR, MAXIT>(buf, g, tw, epi); break;
-        Q3B_FFT_SIZES(Q3B_S2)
-#undef Q3B_S2
+#define Q3B_B(N) \
+    case N:                                                 \
+        if constexpr (N <= MAXR) pass_b<N, DIR>(buf, g, tw); \
+        break;
+        Q3B_FFT_SIZES(Q3B_B)
+#undef Q3B_B
         default: break;
     }
 }
 
-// Transform all lines.  Ends with a barrier.  When nb == 1 the first step is
-// the whole transform and the second only applies the epilogue.
-template <int DIR, int MAXIT, typename T, typename Epi>
-__device__ __forceinline__ void lines(T* buf, const LineGeom& g, const T* tw, const Epi& epi) {
-    run_step1<DIR>(buf, g, tw);
+// Backward transform of every line: natural order in, digit-reversed out.
+// Ends with a barrier.
+template <int MAXR, typename T>
+__device__ __forceinline__ void backward(T* buf, const LineGeom& g, const T* tw) {
+    run_a<+1, MAXR>(buf, g, tw);
     __syncthreads();
-    run_step2<DIR, MAXIT>(buf, g, tw, epi);
+    run_b<+1, MAXR>(buf, g, tw);
+    __syncthreads();
+}
+
+// Forward transform of every line: digit-reversed order in, natural out.
+// Ends with a barrier.
+template <int MAXR, typename T>
+__device__ __forceinline__ void forward(T* buf, const LineGeom& g, const T* tw) {
+    run_b<-1, MAXR>(buf, g, tw);
+    __syncthreads();
+    run_a<-1, MAXR>(buf, g, tw);
+    __syncthreads();
+}
+
+// Backward transform, epi(line, natural index, value) on every value, forward
+// transform; natural order in and out.  Three passes, ends with a barrier.
+template <int MAXR, typename T, typename Epi>
+__device__ __forceinline__ void roundtrip(T* buf, const LineGeom& g, const T* tw, const Epi& epi) {
+    run_a<+1, MAXR>(buf, g, tw);
+    __syncthreads();
+    switch (g.nb) {
+#define Q3B_M(N) \
+    case N:                                                   \
+        if constexpr (N <= MAXR) pass_mid<N>(buf, g, tw, epi); \
+        break;
+        Q3B_FFT_SIZES(Q3B_M)
+#undef Q3B_M
+        default: break;
+    }
+    __syncthreads();
+    run_a<-1, MAXR>(buf, g, tw);
+    __syncthreads();
 }
 
 }  // namespace fft

@@ -15,19 +15,25 @@ namespace q3b {
 namespace {
 
 constexpr int kStickThreads = 256;
-constexpr int kPlaneThreads = 256;
 
+// V/N of one plane in the layout the plane kernel meets it: [w1][w2 position]
+// with the w2 positions of the digit-reversed order the row transform leaves.
 template <typename R> struct VEpilogue {
-    const R* vp;  // V/N of this plane, [w1][w2]
+    const R* vp;
     int n2;
     template <typename T> __device__ __forceinline__ T operator()(int l, int j, T v) const {
-        const R s = vp[j * n2 + l];
-        return s * v;
+        return vp[j * n2 + l] * v;
     }
 };
 
-// pass A: scatter + backward transform along w3, store X[band][w3][stick]
-template <typename R>
+// Kernels are instantiated twice: for lines whose factors are all <= 10
+// (MAXR 10, within 64 registers a thread in FP32) and for any supported line
+// (MAXR 16).
+constexpr int kSmallR = 10;
+
+// pass A: scatter + backward transform along w3, store X[band][w3 pos][stick]
+// (w3 in the transform's digit-reversed order, which pass C undoes)
+template <typename R, int MAXR>
 __global__ void __launch_bounds__(kStickThreads)
 sticks_backward(LocalPlan<R> p, const cplx_t<R>* __restrict__ psi, long ldpsi, cplx_t<R>* X) {
     using T = cplx_t<R>;
@@ -47,7 +53,7 @@ sticks_backward(LocalPlan<R> p, const cplx_t<R>* __restrict__ psi, long ldpsi, c
     }
     __syncthreads();
     fft::LineGeom g{p.n3, p.na3, p.nb3, ns, p.p3, 1, nullptr};
-    fft::lines<+1, 2>(lines, g, tw, fft::NoEpilogue{});
+    fft::backward<MAXR>(lines, g, tw);
     T* xb = X + (long)band * p.n3 * p.nsticks;
     for (int idx = threadIdx.x; idx < ns * p.n3; idx += blockDim.x) {
         const int s = idx % ns, i3 = idx / ns;
@@ -55,11 +61,18 @@ sticks_backward(LocalPlan<R> p, const cplx_t<R>* __restrict__ psi, long ldpsi, c
     }
 }
 
-// pass B: one (band, w3) plane per block.  MI = items of the second line step
-// a thread holds at once: more per thread means fewer barrier rounds but more
-// registers (fewer resident blocks); the autotuner picks it per plan.
-template <typename R, int MI>
-__global__ void __launch_bounds__(kPlaneThreads) planes(LocalPlan<R> p, cplx_t<R>* X) {
+// pass B: one (band, w3) plane per block of NT threads: rows backward (their
+// w2 left digit-reversed), columns backward, V, columns forward (fused round
+// trip), rows forward.  Every pass is in place; one barrier between passes.
+// Register budget: 64 per thread in FP32 (four 256-thread planes of an 80x80
+// grid fit an SM's shared memory), 128 in FP64.
+template <typename R, int NT, int MAXR> constexpr int plane_min_blocks() {
+    constexpr int regs = MAXR <= kSmallR ? (sizeof(R) == 4 ? 64 : 128) : (sizeof(R) == 4 ? 96 : 168);
+    return 65536 / (NT * regs) > 0 ? 65536 / (NT * regs) : 1;
+}
+
+template <typename R, int NT, int MAXR>
+__global__ void __launch_bounds__(NT, (plane_min_blocks<R, NT, MAXR>())) planes(LocalPlan<R> p, cplx_t<R>* X) {
     using T = cplx_t<R>;
     extern __shared__ __align__(16) unsigned char smem[];
     T* tw1 = reinterpret_cast<T*>(smem);
@@ -67,25 +80,24 @@ __global__ void __launch_bounds__(kPlaneThreads) planes(LocalPlan<R> p, cplx_t<R
     T* plane = tw2 + p.n2;
     int* rowb = reinterpret_cast<int*>(plane + (long)p.n1 * p.p2);
     const int i3 = blockIdx.x, band = blockIdx.y;
-    for (int i = threadIdx.x; i < p.n1; i += blockDim.x) tw1[i] = p.tw1[i];
-    for (int i = threadIdx.x; i < p.n2; i += blockDim.x) tw2[i] = p.tw2[i];
-    for (int i = threadIdx.x; i < p.nrows; i += blockDim.x) rowb[i] = p.row_base[i];
-    for (int i = threadIdx.x; i < p.n1 * p.p2; i += blockDim.x) plane[i] = czero<T>();
+    for (int i = threadIdx.x; i < p.n1; i += NT) tw1[i] = p.tw1[i];
+    for (int i = threadIdx.x; i < p.n2; i += NT) tw2[i] = p.tw2[i];
+    for (int i = threadIdx.x; i < p.nrows; i += NT) rowb[i] = p.row_base[i];
+    for (int i = threadIdx.x; i < p.n1 * p.p2; i += NT) plane[i] = czero<T>();
     __syncthreads();
     T* xp = X + ((long)band * p.n3 + i3) * p.nsticks;
-    for (int s = threadIdx.x; s < p.nsticks; s += blockDim.x) plane[p.stick_pos[s]] = xp[s];
+    for (int s = threadIdx.x; s < p.nsticks; s += NT) plane[p.stick_pos[s]] = xp[s];
     __syncthreads();
     fft::LineGeom gr{p.n2, p.na2, p.nb2, p.nrows, 0, 1, rowb};
     fft::LineGeom gc{p.n1, p.na1, p.nb1, p.n2, 1, p.p2, nullptr};
-    fft::lines<+1, MI>(plane, gr, tw2, fft::NoEpilogue{});
-    fft::lines<+1, MI>(plane, gc, tw1, VEpilogue<R>{p.vplane + (long)i3 * p.n1 * p.n2, p.n2});
-    fft::lines<-1, MI>(plane, gc, tw1, fft::NoEpilogue{});
-    fft::lines<-1, MI>(plane, gr, tw2, fft::NoEpilogue{});
-    for (int s = threadIdx.x; s < p.nsticks; s += blockDim.x) xp[s] = plane[p.stick_pos[s]];
+    fft::backward<MAXR>(plane, gr, tw2);
+    fft::roundtrip<MAXR>(plane, gc, tw1, VEpilogue<R>{p.vplane + (long)i3 * p.n1 * p.n2, p.n2});
+    fft::forward<MAXR>(plane, gr, tw2);
+    for (int s = threadIdx.x; s < p.nsticks; s += NT) xp[s] = plane[p.stick_pos[s]];
 }
 
 // pass C: forward transform along w3, gather the sphere, add the kinetic term
-template <typename R>
+template <typename R, int MAXR>
 __global__ void __launch_bounds__(kStickThreads)
 sticks_forward(LocalPlan<R> p, const cplx_t<R>* __restrict__ X, const cplx_t<R>* __restrict__ psi,
                long ldpsi, cplx_t<R>* hpsi, long ldh) {
@@ -104,7 +116,7 @@ sticks_forward(LocalPlan<R> p, const cplx_t<R>* __restrict__ X, const cplx_t<R>*
     }
     __syncthreads();
     fft::LineGeom g{p.n3, p.na3, p.nb3, ns, p.p3, 1, nullptr};
-    fft::lines<-1, 2>(lines, g, tw, fft::NoEpilogue{});
+    fft::forward<MAXR>(lines, g, tw);
     const T* ps = psi + (long)band * ldpsi;
     T* hs = hpsi + (long)band * ldh;
     const int e0 = p.stick_start[s0], e1 = p.stick_start[s0 + ns];
@@ -133,16 +145,30 @@ template <typename R> size_t stick_smem_bytes(const LocalPlan<R>& p) {
     return (size_t)(p.n3 + p.sg * p.p3) * sizeof(cplx_t<R>);
 }
 
+template <typename R, int MAXR> void set_limits_for() {
+    const int lim = 227 * 1024;
+    const void* pk[3] = {reinterpret_cast<const void*>(planes<R, 128, MAXR>),
+                         reinterpret_cast<const void*>(planes<R, 256, MAXR>),
+                         reinterpret_cast<const void*>(planes<R, 512, MAXR>)};
+    for (const void* k : pk) {
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    }
+    cudaFuncSetAttribute(sticks_backward<R, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(sticks_forward<R, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+}
+
 template <typename R> void set_smem_limits() {
     static std::once_flag once;
     std::call_once(once, [] {
-        const int lim = 227 * 1024;
-        cudaFuncSetAttribute(planes<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-        cudaFuncSetAttribute(planes<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-        cudaFuncSetAttribute(planes<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-        cudaFuncSetAttribute(sticks_backward<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-        cudaFuncSetAttribute(sticks_forward<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        set_limits_for<R, kSmallR>();
+        set_limits_for<R, 16>();
     });
+}
+
+template <typename R, int NT, int MAXR>
+void launch_planes(dim3 grid, size_t smem, cudaStream_t st, const LocalPlan<R>& p, cplx_t<R>* X) {
+    planes<R, NT, MAXR><<<grid, NT, smem, st>>>(p, X);
 }
 
 }  // namespace
@@ -197,21 +223,32 @@ void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, l
         cplx_t<R>* hs = hpsi + (long)b0 * ldh;
         if (p.nsticks > 0) {
             if (tm) tm->begin(PhaseTimer::STICKS_BACKWARD);
-            sticks_backward<R><<<dim3(nsg, nb), kStickThreads, smem_s, st>>>(p, ps, ldpsi, X);
+            const bool small3 = p.na3 <= kSmallR && p.nb3 <= kSmallR;
+            if (small3)
+                sticks_backward<R, kSmallR><<<dim3(nsg, nb), kStickThreads, smem_s, st>>>(p, ps, ldpsi, X);
+            else
+                sticks_backward<R, 16><<<dim3(nsg, nb), kStickThreads, smem_s, st>>>(p, ps, ldpsi, X);
             Q3B_LAUNCH_CHECK();
             if (tm) tm->end();
             if (tm) tm->begin(PhaseTimer::PLANES);
             const dim3 gp(p.n3, nb);
-            if (p.plane_items >= 4 && !std::is_same<R, double>::value)
-                planes<R, 4><<<gp, kPlaneThreads, smem_p, st>>>(p, X);
-            else if (p.plane_items >= 2)
-                planes<R, 2><<<gp, kPlaneThreads, smem_p, st>>>(p, X);
-            else
-                planes<R, 1><<<gp, kPlaneThreads, smem_p, st>>>(p, X);
+            const bool small12 = p.na1 <= kSmallR && p.nb1 <= kSmallR && p.na2 <= kSmallR && p.nb2 <= kSmallR;
+            if (small12) {
+                if (p.plane_threads >= 512) launch_planes<R, 512, kSmallR>(gp, smem_p, st, p, X);
+                else if (p.plane_threads >= 256) launch_planes<R, 256, kSmallR>(gp, smem_p, st, p, X);
+                else launch_planes<R, 128, kSmallR>(gp, smem_p, st, p, X);
+            } else {
+                if (p.plane_threads >= 512) launch_planes<R, 512, 16>(gp, smem_p, st, p, X);
+                else if (p.plane_threads >= 256) launch_planes<R, 256, 16>(gp, smem_p, st, p, X);
+                else launch_planes<R, 128, 16>(gp, smem_p, st, p, X);
+            }
             Q3B_LAUNCH_CHECK();
             if (tm) tm->end();
             if (tm) tm->begin(PhaseTimer::STICKS_FORWARD);
-            sticks_forward<R><<<dim3(nsg, nb), kStickThreads, smem_s, st>>>(p, X, ps, ldpsi, hs, ldh);
+            if (small3)
+                sticks_forward<R, kSmallR><<<dim3(nsg, nb), kStickThreads, smem_s, st>>>(p, X, ps, ldpsi, hs, ldh);
+            else
+                sticks_forward<R, 16><<<dim3(nsg, nb), kStickThreads, smem_s, st>>>(p, X, ps, ldpsi, hs, ldh);
             Q3B_LAUNCH_CHECK();
             if (tm) tm->end();
         }

@@ -26,7 +26,7 @@ template <typename R> struct LocalPlan {
     int p3;             // pitch of a stick line in shared memory (odd)
     int na1, nb1, na2, nb2, na3, nb3;
     int sg;             // sticks per block in passes A and C
-    int plane_items;    // second-step items per thread in the plane kernel (1, 2, 4)
+    int plane_threads;  // threads per block of the plane kernel (128, 256, 512)
     int nunmapped;      // G outside the grid: kinetic term only
     const int* stick_start;  // nsticks+1, ranges into the entry arrays
     const int* entry_g;      // G index (caller's order) of each sphere entry
@@ -39,7 +39,8 @@ template <typename R> struct LocalPlan {
     const T* tw2;
     const T* tw3;
     const R* ke;             // |k+G|^2 (Ry), caller's order
-    const R* vplane;         // V(r)/N laid out [w3][w1][w2]
+    const R* vplane;         // V(r)/N laid out [w3 pos][w1][w2 pos], with the w3 and w2
+                             // positions of the backward transform's digit-reversed order
 };
 
 // bytes of the stick buffer per band

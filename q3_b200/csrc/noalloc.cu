@@ -17,6 +17,8 @@
 // array and the last call's contents stay in it; every element a call reads
 // it has written first in that call, so nothing needs clearing, but calls
 // whose work overlaps on the GPU (other streams, other threads) race on it.
+#include <mutex>
+
 #include "context.cuh"
 #include "q3b.h"
 
@@ -30,7 +32,9 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
 
 void* scratch_address(int device) {
     static void* addr[kMaxDevices] = {};
+    static std::mutex mu;
     if (device < 0 || device >= kMaxDevices) throw Status(Q3B_ERR_INVALID, "device index out of range");
+    std::lock_guard<std::mutex> lk(mu);
     if (!addr[device]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);

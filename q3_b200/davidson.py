@@ -30,6 +30,7 @@ class SolveResult:
     max_residual_norm: float
     seconds: float
     stage_ms: dict
+    fp64_seconds: float
 
 
 class PlanewaveDavidsonDiagonalizer:
@@ -85,7 +86,8 @@ class PlanewaveDavidsonDiagonalizer:
         check(h, rc)
         stages = dict(zip(DavidsonStats.STAGES, list(st.stage_ms)))
         return SolveResult(eig, out, st.iterations, st.fp64_iterations, st.h_applications,
-                           st.unconverged, st.collapses, st.max_residual_norm, st.seconds, stages)
+                           st.unconverged, st.collapses, st.max_residual_norm, st.seconds, stages,
+                           st.fp64_seconds)
 
 
 def hegv(applicator, h: np.ndarray, s: np.ndarray):

@@ -1,0 +1,133 @@
+"""Band-solve serving over libq3b's server (continuous batching on one GPU).
+
+``BandSolveServer`` wraps ``q3b_server_*``: requests (one cell at one k-point,
+built by ``q3_b200.synthetic``) are submitted as they arrive, admitted by an
+HBM budget, solved concurrently on separate streams, and collected with their
+queue, solve and end-to-end latencies.  ``run_poisson_stream`` drives a
+seeded Poisson arrival process and reports p50/p99 latency and solves/s.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import time
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import FP64, MIXED, DavidsonOpts, DavidsonStats, Request, RequestTimes
+
+
+@dataclasses.dataclass
+class Served:
+    id: int
+    eigenvalues: np.ndarray
+    bands: np.ndarray
+    iterations: int
+    fp64_iterations: int
+    unconverged: int
+    queue_ms: float
+    solve_ms: float
+    latency_ms: float
+    estimated_bytes: int
+
+
+class BandSolveServer:
+    def __init__(self, device: int = 0, hbm_budget: int = 0, workers: int = 4):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        rc = self.lib.q3b_server_create(int(device), int(hbm_budget), int(workers), C.byref(h))
+        if rc != 0:
+            raise _lib.Q3BError(rc, "cannot create a server")
+        self.h = h.value
+        self._shape: Dict[int, tuple] = {}
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.q3b_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            msg = self.lib.q3b_server_last_error(self.h)
+            raise _lib.Q3BError(rc, msg.decode() if msg else "")
+
+    def submit(self, system, k: int = 0, tolerance: float = 1e-8, max_iterations: int = 100,
+               precision: int = FP64, mixed_tolerance: float = 1e-6, refine_sweeps: int = 100,
+               bands: Optional[np.ndarray] = None) -> int:
+        """Queue one band solve of `system` at k-point `k`; returns its id."""
+        kp = system.kpoints[k]
+        n1, n2, n3 = system.cell.grid
+        v = np.ascontiguousarray(system.v_r, dtype=np.float64)
+        g2g = np.ascontiguousarray(kp.g_to_grid, dtype=np.int32)
+        ke = np.ascontiguousarray(kp.ke, dtype=np.float64)
+        beta = np.asfortranarray(kp.beta, dtype=np.complex128)
+        offs = np.ascontiguousarray(kp.atom_proj_offsets, dtype=np.int32)
+        dblk = np.ascontiguousarray(kp.d_blocks, dtype=np.float64)
+        psi = np.asfortranarray(system.psi0[k] if bands is None else bands, dtype=np.complex128)
+        opts = DavidsonOpts()
+        self.lib.q3b_davidson_default_opts(C.byref(opts))
+        opts.tolerance = tolerance
+        opts.max_iterations = max_iterations
+        opts.precision = precision
+        opts.mixed_tolerance = mixed_tolerance
+        opts.refine_sweeps = refine_sweeps
+        req = Request(n1, n2, n3, v.ctypes.data, kp.npw, g2g.ctypes.data, ke.ctypes.data, kp.nproj,
+                      beta.ctypes.data, len(offs) - 1, offs.ctypes.data, dblk.ctypes.data,
+                      system.nbands, psi.ctypes.data, None, C.pointer(opts))
+        rid = C.c_int()
+        self._check(self.lib.q3b_server_submit(self.h, C.byref(req), C.byref(rid)))
+        self._shape[rid.value] = (kp.npw, system.nbands)
+        return rid.value
+
+    def done(self, rid: int) -> bool:
+        return self.lib.q3b_server_poll(self.h, rid) == 1
+
+    def wait(self, rid: int) -> Served:
+        npw, nb = self._shape.pop(rid)
+        bands = np.empty((npw, nb), dtype=np.complex128, order="F")
+        eig = np.empty(nb, dtype=np.float64)
+        st = DavidsonStats()
+        tm = RequestTimes()
+        self._check(self.lib.q3b_server_wait(self.h, rid, bands.ctypes.data, eig.ctypes.data,
+                                             C.byref(st), C.byref(tm)))
+        return Served(rid, eig, bands, st.iterations, st.fp64_iterations, st.unconverged,
+                      tm.queue_ms, tm.solve_ms, tm.latency_ms, tm.estimated_bytes)
+
+
+def run_poisson_stream(server: BandSolveServer, systems: Sequence, rate_hz: float, seed: int = 1238,
+                       **solve_kw) -> Dict:
+    """Submit `systems` at seeded Poisson arrival times; collect every result.
+
+    Returns p50/p99 latency (ms), solves/s over the stream and the results."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate_hz, size=len(systems))
+    t0 = time.perf_counter()
+    ids: List[int] = []
+    next_t = 0.0
+    for sy, gap in zip(systems, gaps):
+        next_t += gap
+        delay = next_t - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(server.submit(sy, **solve_kw))
+    results = [server.wait(i) for i in ids]
+    wall = time.perf_counter() - t0
+    lat = np.array([r.latency_ms for r in results])
+    return {
+        "requests": len(results),
+        "p50_ms": float(np.percentile(lat, 50)),
+        "p99_ms": float(np.percentile(lat, 99)),
+        "mean_queue_ms": float(np.mean([r.queue_ms for r in results])),
+        "solves_per_s": len(results) / wall,
+        "wall_s": wall,
+        "unconverged_requests": int(sum(1 for r in results if r.unconverged)),
+        "results": results,
+    }

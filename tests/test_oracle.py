@@ -165,3 +165,32 @@ def test_oracle_davidson_seeds_from_kinetic_energy():
     exact = np.linalg.eigvalsh(hd)[:5]
     res = davidson.solve(lambda x: hd @ x, kp.ke, None, 5, tolerance=1e-11, max_iterations=80)
     assert np.max(np.abs(res.eigenvalues - exact)) < 1e-9
+
+
+def test_starting_rotation_oracle_matches_reference_kat():
+    """The reference's StartingSubspaceSolver test (test_starting_subspace_solver_gpu.cpp:
+    61-145): diagonal H_gg = 1 + g/2, 37 plane waves, 5 vectors with its sin/cos
+    formula; projections and rotation equal the direct sums.  Then the whole
+    rotation: Ritz values bound the exact eigenvalues of H from above."""
+    from oracle import starting as ostart
+    npw, nvec, nb = 37, 5, 3
+    g = np.arange(npw)[:, None]
+    v = np.arange(nvec)[None, :]
+    chi = np.sin(0.3 * (g + 1) * (v + 1)) + 1j * np.cos(0.7 * (g + 2) + 0.2 * v)
+    diag = 1.0 + 0.5 * np.arange(npw)
+    h, s = ostart.project(lambda x: diag[:, None] * x, chi)
+    for i in range(nvec):
+        for j in range(nvec):
+            eh = sum(diag[q] * np.conj(chi[q, i]) * chi[q, j] for q in range(npw))
+            es = sum(np.conj(chi[q, i]) * chi[q, j] for q in range(npw))
+            assert abs(h[i, j] - eh) < 1e-11 and abs(s[i, j] - es) < 1e-11
+    b = np.arange(nb)[None, :]
+    vv = np.arange(nvec)[:, None]
+    coef = (0.1 * (vv + 1) - 0.05 * b) + 1j * (0.03 * (b + 1) * (vv - 2))
+    bands = ostart.rotate_into_bands(chi, coef, nb)
+    for bb in range(nb):
+        for q in range(npw):
+            assert abs(bands[q, bb] - sum(chi[q, k] * coef[k, bb] for k in range(nvec))) < 1e-12
+    w, bands = ostart.starting_subspace(lambda x: diag[:, None] * x, chi, nb)
+    assert np.all(w >= diag[:nb] - 1e-12)
+    assert np.max(np.abs(bands.conj().T @ bands - np.eye(nb))) < 1e-12
