@@ -1,4 +1,7 @@
 // q3b context: HBM accounting, potential, k-point plan, H|psi> orchestration.
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cmath>
 #include <atomic>
 #include <type_traits>
@@ -331,6 +334,15 @@ template <typename R> int Context::sticks_chunk(int nvec) const {
     return static_cast<int>(c);
 }
 
+// Tuning results by (grid, precision), shared by every context of the process:
+// the best block size of the plane kernel depends on the plane's shared-memory
+// footprint and line factors, so a new k-point or request on a grid seen
+// before reuses it instead of timing again.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tuned;
+}  // namespace
+
 template <typename R> void Context::tune_local() {
     using T = cplx_t<R>;
     bool& done = std::is_same<R, double>::value ? kp.tuned64 : kp.tuned32;
@@ -338,6 +350,15 @@ template <typename R> void Context::tune_local() {
     done = true;
     LocalPlan<R>& lp = const_cast<LocalPlan<R>&>(local_plan<R>());
     if (lp.nsticks == 0) return;
+    const auto key = std::make_tuple(lp.n1, lp.n2, lp.n3, (int)sizeof(R));
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            lp.plane_threads = it->second;
+            return;
+        }
+    }
     const int nb = 16;
     const size_t n = (size_t)kp.npw * nb;
     ws_tune.reserve(this, 2 * n * sizeof(T));
@@ -370,6 +391,10 @@ template <typename R> void Context::tune_local() {
         }
     }
     lp.plane_threads = best_threads;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned[key] = best_threads;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     ws_tune.release();

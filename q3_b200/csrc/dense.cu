@@ -3,17 +3,18 @@
 // potrf : blocked right-looking upper Cholesky (32x32 blocks): a diagonal
 //         block factor + its triangular inverse, a panel solve and a trailing
 //         update per block step.
-// trtri : U^{-1} block column by block column, each a set of independent
-//         block products.
+// trtri : U^{-1} by recursive doubling: the diagonal blocks' inverses, then
+//         per level the off-diagonal block of each pair, -Inv11 U12 Inv22, as
+//         two batched tile products.
 // hegv  : H c = w S c reduced to C = U^{-H} H U^{-1} with S = U^H U, as
 //         zhegv does (subspace/serial.hpp:18-151 calls zhegv itype 1), solved
 //         by heev, back-transformed c = U^{-1} z.
-// heev  : Householder tridiagonalisation in one cooperative kernel (two grid
-//         barriers per column, each wait bounded), the complex subdiagonal
+// heev  : Householder tridiagonalisation in one cooperative kernel (one grid
+//         barrier per column, each wait bounded), the complex subdiagonal
 //         made real by a diagonal phase, eigenvalues by multisection on
-//         Sturm counts (one warp per eigenvalue), eigenvectors by inverse
-//         iteration with Gram-Schmidt inside clusters of close eigenvalues,
-//         then the reflectors applied back (one warp per vector).
+//         division-free Sturm counts (one warp per eigenvalue), eigenvectors
+//         by inverse iteration in shared memory with Gram-Schmidt inside
+//         clusters of close eigenvalues, then Z = Q (phase * Y) by GEMM.
 #include <algorithm>
 #include <cmath>
 #include <mutex>
@@ -49,13 +50,30 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Diagonal block k, 32x32 threads: warp c, lane r owns element (r, c).  At
 // step j every (r, c) with j < r <= c subtracts conj(G(j,r)) G(j,c) / G(j,j)
 // (row j of U times its conjugate, taken from the unscaled row) while row j
-// is scaled into U: one barrier a step.  Then U^{-1} a column per warp: lane t
-// holds X(t, c) and row r, from the bottom up, is a warp sum.
-__global__ void __launch_bounds__(1024)
+// is scaled into U: one barrier a step.  The thread that finishes a pivot
+// (the diagonal element of the next step) also forms its reciprocal, square
+// root and reciprocal square root, so no step waits on a division.  Then
+// U^{-1} a column per warp: lane t holds X(t, c) and row r, from the bottom
+// up, is a warp sum.
+__device__ __forceinline__ void pivot_terms(double piv, int j, int bs, int r0, double* rp, double* sq,
+                                            double* isq, int* bad) {
+    if (!(piv > 0.0)) {
+        if (j < bs) atomicMin(bad, r0 + j + 1);
+        piv = 1.0;
+    }
+    const double q = sqrt(piv);
+    rp[j] = 1.0 / piv;
+    sq[j] = q;
+    isq[j] = 1.0 / q;
+}
+
+__global__ void __launch_bounds__(1024, 1)
 potrf_diag(int n, int k, double2* A, int lda, double2* dinv, int* info) {
     if (vload(info)) return;
     __shared__ double2 a[NB][NB + 1];  // a[c][r] = G(r, c)
     __shared__ double2 u[NB][NB + 1];  // u[c][r] = U(r, c)
+    __shared__ double s_rp[NB], s_sq[NB], s_isq[NB];
+    __shared__ int s_bad;
     const int r = threadIdx.x & 31, c = threadIdx.x >> 5;
     const int r0 = k * NB;
     const int bs = min(NB, n - r0);
@@ -64,22 +82,22 @@ potrf_diag(int n, int k, double2* A, int lda, double2* dinv, int* info) {
         if (r < bs && c < bs && r <= c) v = A[(r0 + r) + (long)(r0 + c) * lda];
         a[c][r] = v;
         u[c][r] = mk(0.0, 0.0);
+        if (threadIdx.x == 0) s_bad = 0x7fffffff;
     }
     __syncthreads();
-    int bad = 0;
+    if (threadIdx.x == 0) pivot_terms(a[0][0].x, 0, bs, r0, s_rp, s_sq, s_isq, &s_bad);
+    __syncthreads();
     for (int j = 0; j < NB; ++j) {
-        double piv = a[j][j].x;
-        if (!(piv > 0.0)) {
-            if (!bad && j < bs) bad = r0 + j + 1;
-            piv = 1.0;
-        }
         if (r == j && c >= j) {
-            const double us = sqrt(piv);
-            u[c][j] = (c == j) ? mk(us, 0.0) : mk(a[c][j].x / us, a[c][j].y / us);
+            const double is = s_isq[j];
+            u[c][j] = (c == j) ? mk(s_sq[j], 0.0) : mk(a[c][j].x * is, a[c][j].y * is);
         }
         if (j < r && r <= c) {
             const double2 g = cmulc(a[r][j], a[c][j]);  // conj(G(j,r)) G(j,c)
-            a[c][r] = a[c][r] - mk(g.x / piv, g.y / piv);
+            const double rp = s_rp[j];
+            const double2 v = a[c][r] - mk(g.x * rp, g.y * rp);
+            a[c][r] = v;
+            if (r == c && r == j + 1) pivot_terms(v.x, j + 1, bs, r0, s_rp, s_sq, s_isq, &s_bad);
         }
         __syncthreads();
     }
@@ -90,13 +108,13 @@ potrf_diag(int n, int k, double2* A, int lda, double2* dinv, int* info) {
         p = warp_sum(p);
         if (r == rr) {
             const double2 rhs = (rr == c) ? mk(1.0 - p.x, -p.y) : mk(-p.x, -p.y);
-            const double ud = u[rr][rr].x;
-            x = mk(rhs.x / ud, rhs.y / ud);
+            const double iu = s_isq[rr];
+            x = mk(rhs.x * iu, rhs.y * iu);
         }
     }
     if (r < bs && c < bs && r <= c) A[(r0 + r) + (long)(r0 + c) * lda] = u[c][r];
     dinv[(long)k * NB * NB + r + c * NB] = x;
-    if (threadIdx.x == 0 && bad) atomicCAS(info, 0, bad);
+    if (threadIdx.x == 0 && s_bad != 0x7fffffff) atomicCAS(info, 0, s_bad);
 }
 
 // U(k, j) = U_kk^{-H} G(k, j) for every block column j > k
@@ -159,50 +177,76 @@ __global__ void trtri_diag(int n, const double2* dinv, double2* U) {
     }
 }
 
-// Uinv(i, j) = -[sum_{t=i}^{j-1} Uinv(i, t) U(t, j)] X_j for all i < j
+// One level of the recursive triangular inverse.  At level m the diagonal
+// blocks of order m are inverted already; pair p joins blocks [r1, r1+m) and
+// [r2, r2+m2) (r1 = 2mp, r2 = r1 + m, m2 = min(m, n - r2)) through
+//   inv([U11 U12; 0 U22]) = [Inv11, -Inv11 U12 Inv22; 0, Inv22]:
+// mode 0 forms T_p = U12 Inv22 (m x m2, ld m, in T), mode 1 writes
+// Inv12 = -Inv11 T_p into Ui.  Block (blockIdx.y, blockIdx.z) is a 32x32 tile
+// of the product; K runs over 32-chunks, skipping the zero chunks of the
+// triangular factor, with the next chunk's tiles loaded into registers while
+// the current one is multiplied.
 __global__ void __launch_bounds__(256)
-trtri_col(int n, int j, const double2* A, int lda, const double2* dinv, double2* Ui) {
-    const int i = blockIdx.x;
-    __shared__ double2 p[NB][NB + 1];  // p[q][r] = Uinv(i_r, t_q)
-    __shared__ double2 u[NB][NB + 1];  // u[c][q] = U(t_q, j_c)
+trtri_level(int n, int m, int mode, const double2* U, int ldu, double2* Ui, double2* T) {
+    const int p = blockIdx.x, ti = blockIdx.y, tj = blockIdx.z;
+    const int r1 = 2 * m * p, r2 = r1 + m;
+    const int m2 = min(m, n - r2);
+    if (m2 <= 0 || tj * NB >= m2) return;
+    __shared__ double2 sa[NB][NB + 1];  // sa[k][i] = A(i, k)
+    __shared__ double2 sb[NB][NB + 1];  // sb[j][k] = B(k, j)
+    double2* Tp = T + (size_t)p * m * m;
+    const int kmax = (mode == 0) ? m2 : m;
+    const int kc0 = (mode == 0) ? 0 : ti;                               // Inv11 upper triangular
+    const int kc1 = (mode == 0) ? min(tj, (m2 - 1) / NB) : (kmax - 1) / NB;  // Inv22 upper triangular
     const int tid = threadIdx.x;
-    const int bsi = min(NB, n - i * NB), bsj = min(NB, n - j * NB);
-    double2 acc[4];
+    auto a_at = [&](int i, int k) -> double2 {
+        if (k >= kmax) return mk(0.0, 0.0);
+        return mode == 0 ? U[(r1 + i) + (long)(r2 + k) * ldu] : Ui[(r1 + i) + (long)(r1 + k) * n];
+    };
+    auto b_at = [&](int k, int j) -> double2 {
+        if (k >= kmax || j >= m2) return mk(0.0, 0.0);
+        return mode == 0 ? Ui[(r2 + k) + (long)(r2 + j) * n] : Tp[k + (long)j * m];
+    };
+    double2 ra[4], rb[4], acc[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc[q] = mk(0.0, 0.0);
-    for (int t = i; t < j; ++t) {
-        const int bst = min(NB, n - t * NB);
+    for (int q = 0; q < 4; ++q) {
+        acc[q] = mk(0.0, 0.0);
+        const int idx = tid + q * 256, x = idx % NB, y = idx / NB;
+        ra[q] = (kc0 <= kc1) ? a_at(ti * NB + x, kc0 * NB + y) : mk(0.0, 0.0);
+        rb[q] = (kc0 <= kc1) ? b_at(kc0 * NB + x, tj * NB + y) : mk(0.0, 0.0);
+    }
+    for (int kc = kc0; kc <= kc1; ++kc) {
         __syncthreads();
-        for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-            const int r = idx % NB, q = idx / NB;
-            p[q][r] = (r < bsi && q < bst) ? Ui[(i * NB + r) + (long)(t * NB + q) * n] : mk(0.0, 0.0);
-            u[r][q] = (q < bst && r < bsj) ? A[(t * NB + q) + (long)(j * NB + r) * lda] : mk(0.0, 0.0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int idx = tid + q * 256, x = idx % NB, y = idx / NB;
+            sa[y][x] = ra[q];
+            sb[y][x] = rb[q];
         }
         __syncthreads();
+        if (kc < kc1) {
 #pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const int idx = tid + s * 256;
-            const int r = idx % NB, c = idx / NB;
-            double2 a = acc[s];
-            for (int q = 0; q < NB; ++q) a = a + cmul(p[q][r], u[c][q]);
-            acc[s] = a;
+            for (int q = 0; q < 4; ++q) {
+                const int idx = tid + q * 256, x = idx % NB, y = idx / NB;
+                ra[q] = a_at(ti * NB + x, (kc + 1) * NB + y);
+                rb[q] = b_at((kc + 1) * NB + x, tj * NB + y);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int idx = tid + q * 256, i = idx % NB, j = idx / NB;
+            double2 v = acc[q];
+#pragma unroll 8
+            for (int k = 0; k < NB; ++k) v = v + cmul(sa[k][i], sb[j][k]);
+            acc[q] = v;
         }
     }
-    __syncthreads();
-    // p <- acc, u <- X_j
-    for (int s = 0; s < 4; ++s) {
-        const int idx = tid + s * 256;
-        const int r = idx % NB, c = idx / NB;
-        p[c][r] = acc[s];
-        u[c][r] = dinv[(long)j * NB * NB + r + c * NB];
-    }
-    __syncthreads();
-    for (int s = 0; s < 4; ++s) {
-        const int idx = tid + s * 256;
-        const int r = idx % NB, c = idx / NB;
-        double2 a = mk(0.0, 0.0);
-        for (int q = 0; q < NB; ++q) a = a + cmul(p[q][r], u[c][q]);
-        if (r < bsi && c < bsj) Ui[(i * NB + r) + (long)(j * NB + c) * n] = mk(-a.x, -a.y);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int idx = tid + q * 256, i = ti * NB + idx % NB, j = tj * NB + idx / NB;
+        if (i >= m || j >= m2) continue;
+        if (mode == 0) Tp[i + (long)j * m] = acc[q];
+        else Ui[(r1 + i) + (long)(r2 + j) * n] = mk(-acc[q].x, -acc[q].y);
     }
 }
 
@@ -279,22 +323,6 @@ __device__ __forceinline__ bool grid_sync(unsigned* bar, unsigned nblocks, int* 
     return s_ok != 0;
 }
 
-// one thread waits (bounded) for a flag raised with st.release; false when it
-// gave up or another block reported an error
-__device__ __forceinline__ bool wait_flag(const unsigned* flag, int* err) {
-    const long long t0 = clock64();
-    while (true) {
-        unsigned f;
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(f) : "l"(flag) : "memory");
-        if (f != 0u) return true;
-        if (vload(err)) return false;
-        if (clock64() - t0 > (1LL << 32)) {
-            atomicExch(err, 1);
-            return false;
-        }
-    }
-}
-
 // ------------------------------------------------------------------ hetrd
 // A (n x n, ld n, full Hermitian; read once) reduced to tridiagonal form by
 // reflectors H_k = I - tau_k v_k v_k^H on rows/columns k+1..n-1, with
@@ -302,23 +330,26 @@ __device__ __forceinline__ bool wait_flag(const unsigned* flag, int* err) {
 // so that A = Q T Q^H and an eigenvector of A is W^H times one of T.
 // Block b owns columns c = b + G*j (cyclic, G = gridDim.x); it keeps them in
 // shared memory for the whole reduction, and its columns of W too when they
-// fit (`w_in_smem`), else in global memory.  Per column step, one grid
-// barrier, after every block has published its entries of p = tau A v and its
-// share of v^H p; and one flag, set by the owner of column k+1 once it has
-// updated and published that column, which the other blocks wait for before
-// the next step.  p and the shares are double-buffered by step parity: a
-// block can run at most one step ahead of another (the barrier of the next
-// step holds it), so it never overwrites values still being read.  Only
-// column k+1, p and the shares cross blocks, through L2 (ld.global.cg);
-// every wait is bounded.
+// fit (`w_in_smem`), else in global memory.
+//
+// One grid barrier per column step.  Before it, every block publishes its
+// entries of p = tau A v and its share of v^H p, and the owner of column k+1
+// publishes that column as it stands before step k's update.  After it, every
+// block reads the three together (one L2 latency), forms w, and applies step
+// k's rank-2 update to its own copy of column k+1, which is the next step's
+// Householder input: no block waits for another between the barriers.  The
+// published vectors are double-buffered by step parity; a block can run at
+// most one step ahead of another (the next barrier holds it), so nothing is
+// overwritten while it is still being read.  Every wait is bounded.
 __global__ void __launch_bounds__(256, 1)
 hetrd_smem(int n, int cpb, int w_in_smem, const double2* A, double* d, double2* e, double2* W,
-           double2* xbuf, double2* pbuf2, double2* partial2, unsigned* bar, unsigned* ready, int* err) {
+           double2* xpre2, double2* pbuf2, double2* partial2, unsigned* bar, int* err) {
     extern __shared__ __align__(16) unsigned char smem[];
     double2* cols = reinterpret_cast<double2*>(smem);   // cpb columns of A
     double2* sv = cols + (size_t)cpb * n;              // v
     double2* sw = sv + n;                              // w
-    double2* wsm = sw + n;                             // cpb columns of W (if w_in_smem)
+    double2* sx = sw + n;                              // column k, rows k.. (the next v)
+    double2* wsm = sx + n;                             // cpb columns of W (if w_in_smem)
     __shared__ double red[8];
     __shared__ double2 redc[8];
     __shared__ double s_tau;
@@ -335,23 +366,17 @@ hetrd_smem(int n, int cpb, int w_in_smem, const double2* A, double* d, double2* 
             wc[r] = (r == c) ? mk(1.0, 0.0) : mk(0.0, 0.0);
         }
     }
-    if (b == 0)
-        for (int r = tid; r < n; r += blockDim.x) xbuf[r] = A[r];
-    if (!grid_sync(bar, G, err)) return;
-    __shared__ int s_go;
+    for (int r = tid; r < n; r += blockDim.x) sx[r] = A[r];  // column 0
+    __syncthreads();
     for (int k = 0; k + 1 < n; ++k) {
         const int m = n - k - 1;
-        double2* pbuf = pbuf2 + (size_t)(k & 1) * n;
-        double2* partial = partial2 + (size_t)(k & 1) * G;
-        // column k, rows k+1.., as published by its owner (step k-1)
-        if (k > 0 && k % G != b) {
-            if (tid == 0) s_go = wait_flag(ready + k, err);
-            __syncthreads();
-            if (!s_go) return;
-        }
+        const int par = k & 1;
+        double2* pbuf = pbuf2 + (size_t)par * n;
+        double2* partial = partial2 + (size_t)par * G;
+        double2* xpre = xpre2 + (size_t)par * n;
         double part = 0.0;
         for (int j = tid; j < m; j += blockDim.x) {
-            const double2 x = __ldcg(&xbuf[k + 1 + j]);
+            const double2 x = sx[k + 1 + j];
             sv[j] = x;
             if (j > 0) part += x.x * x.x + x.y * x.y;
         }
@@ -374,9 +399,14 @@ hetrd_smem(int n, int cpb, int w_in_smem, const double2* A, double* d, double2* 
             }
             s_tau = t;
             if (b == 0) {
-                d[k] = __ldcg(&xbuf[k]).x;
+                d[k] = sx[k].x;
                 e[k] = alpha;
             }
+        }
+        // the owner of column k+1 publishes it as it stands before this step
+        if ((k + 1) % G == b) {
+            const double2* col = cols + (size_t)((k + 1) / G) * n + (k + 1);
+            for (int j = tid; j < m; j += blockDim.x) xpre[j] = col[j];
         }
         __syncthreads();
         const double tk = s_tau;
@@ -403,20 +433,33 @@ hetrd_smem(int n, int cpb, int w_in_smem, const double2* A, double* d, double2* 
             partial[b] = sacc;
         }
         if (!grid_sync(bar, G, err)) return;
+        // column k+1 before the update, p and the shares, read together
+        for (int j = tid; j < m; j += blockDim.x) {
+            sx[k + 1 + j] = __ldcg(&xpre[j]);
+            if (tk != 0.0) sw[j] = __ldcg(&pbuf[k + 1 + j]);
+        }
+        if (tk != 0.0 && warp == 0) {
+            double2 sacc = mk(0.0, 0.0);
+            for (int q = lane; q < G; q += 32) sacc = sacc + __ldcg(&partial[q]);
+            sacc = warp_sum(sacc);
+            if (lane == 0) redc[0] = sacc;
+        }
+        __syncthreads();
         if (tk != 0.0) {
-            if (warp == 0) {
-                double2 sacc = mk(0.0, 0.0);
-                for (int q = lane; q < G; q += 32) sacc = sacc + __ldcg(&partial[q]);
-                sacc = warp_sum(sacc);
-                if (lane == 0) redc[0] = sacc;
-            }
-            __syncthreads();
             const double half = 0.5 * tk * redc[0].x;  // v^H p is real
             for (int j = tid; j < m; j += blockDim.x) {
-                const double2 p = __ldcg(&pbuf[k + 1 + j]);
+                const double2 p = sw[j];
                 sw[j] = mk(p.x - half * sv[j].x, p.y - half * sv[j].y);
             }
             __syncthreads();
+            // the next step's column: A[k+1+j, k+1] -= v_j conj(w_0) + w_j conj(v_0)
+            {
+                const double2 v0 = sv[0], w0 = sw[0];
+                for (int j = tid; j < m; j += blockDim.x) {
+                    const double2 u = cmul(sv[j], conj2(w0)) + cmul(sw[j], conj2(v0));
+                    sx[k + 1 + j] = sx[k + 1 + j] - u;
+                }
+            }
             for (int jj = warp; jj < owned; jj += 8) {
                 const int i = b + G * jj;
                 // W column: W[k+1:, i'] -= tau v (v^H W[k+1:, i'])
@@ -437,18 +480,9 @@ hetrd_smem(int n, int cpb, int w_in_smem, const double2* A, double* d, double2* 
             }
         }
         __syncthreads();
-        // the owner of column k+1 publishes its rows k+1.. for the next step
-        // and raises its flag; it reads the column from its own shared memory
-        if ((k + 1) % G == b) {
-            const double2* col = cols + (size_t)((k + 1) / G) * n;
-            for (int r = k + 1 + tid; r < n; r += blockDim.x) xbuf[r] = col[r];
-            __threadfence();
-            __syncthreads();
-            if (tid == 0) asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ready + k + 1), "r"(1u) : "memory");
-        }
     }
     if (b == 0 && tid == 0) {
-        if (n < 2 || (n - 1) % G == 0 || wait_flag(ready + n - 1, err)) d[n - 1] = __ldcg(&xbuf[n - 1]).x;
+        d[n - 1] = sx[n - 1].x;
         e[n - 1] = mk(0.0, 0.0);
     }
     if (w_in_smem) {
@@ -527,32 +561,48 @@ __global__ void apply_phase(int n, int nvec, const double2* phase, const double*
     }
 }
 
-// numbers of eigenvalues of the real tridiagonal (d, e2) below x[0..S): S
-// independent recurrences interleaved, so their divisions overlap
+// numbers of eigenvalues of the real tridiagonal (d, e2) below x[0..S).  The
+// count is the number of sign changes along p_0 = 1, p_1, ..., p_n with
+// p_k = (d_k - x) p_{k-1} - e2_{k-1} p_{k-2} (the leading principal minors of
+// T - x I); the ratio p_k / p_{k-1} is the pivot of the LDL^T form, and a
+// ratio below pivmin in magnitude is replaced by -pivmin, as in the LDL^T
+// count.  No division: each step rescales the pair by the power of two of
+// p_{k-1} (exact), which keeps both in range, so the dependent chain per step
+// is one FMA, a select and a multiply.  S independent recurrences interleave.
+__device__ __forceinline__ double pow2_inverse_exponent(double p) {
+    const long long bits = __double_as_longlong(p);
+    const long long e = (bits >> 52) & 0x7ff;
+    return __longlong_as_double((2046 - e) << 52);
+}
+
 template <int S>
 __device__ __forceinline__ void sturm_counts(int n, const double* d, const double* e2, const double* x,
                                              double pivmin, int* c) {
-    double q[S];
+    double p[S], pm[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
-        q[s] = d[0] - x[s];
-        if (fabs(q[s]) < pivmin) q[s] = -pivmin;
-        c[s] = q[s] < 0.0;
+        pm[s] = 1.0;
+        p[s] = d[0] - x[s];
+        if (fabs(p[s]) < pivmin) p[s] = -pivmin;
+        c[s] = p[s] < 0.0;
     }
     for (int k = 1; k < n; ++k) {
         const double dk = d[k], ek = e2[k - 1];
 #pragma unroll
         for (int s = 0; s < S; ++s) {
-            q[s] = (dk - x[s]) - ek / q[s];
-            if (fabs(q[s]) < pivmin) q[s] = -pivmin;
-            c[s] += q[s] < 0.0;
+            const double sc = pow2_inverse_exponent(p[s]);
+            double q = fma(dk - x[s], p[s], -ek * pm[s]);
+            if (fabs(q) < pivmin * fabs(p[s])) q = -pivmin * p[s];
+            c[s] += (q < 0.0) != (p[s] < 0.0);
+            pm[s] = p[s] * sc;
+            p[s] = q * sc;
         }
     }
 }
 
 // one warp per eigenvalue: multisection of [lo, hi] on Sturm counts at
-// 32 x kShifts interior points per round (the interval shrinks 129-fold)
-constexpr int kShifts = 4;
+// 32 x kShifts interior points per round (the interval shrinks 65-fold)
+constexpr int kShifts = 2;
 __global__ void tridiag_multisect(int n, const double* d, const double* e2, const double* bounds, double* w) {
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -781,8 +831,17 @@ __global__ void tridiag_invit_smem(int n, const double* d, const double* ea, con
 constexpr size_t kInvitSmemLimit = 200 * 1024;
 constexpr int kInvitBytesPerRow = 5 * sizeof(double) + 1;
 
+// elements of the recursive inverse's product buffer: the largest level's
+// pairs x m^2
+size_t trtri_tbuf_elems(int n) {
+    size_t most = 0;
+    for (long m = NB; m < n; m *= 2) most = std::max<size_t>(most, (size_t)ceil_div(n, 2 * m) * m * m);
+    return most + 1;
+}
+
 struct Chol {
     double2* dinv;
+    double2* tbuf;  // the recursive inverse's products, n*n/2 at most
     int* info;
 };
 
@@ -790,6 +849,7 @@ Chol chol_take(Scratch& ws, int n) {
     const int nblk = ceil_div(n, NB);
     Chol c;
     c.dinv = ws.take<double2>((size_t)nblk * NB * NB);
+    c.tbuf = ws.take<double2>(trtri_tbuf_elems(n));
     c.info = ws.take<int>(1);
     return c;
 }
@@ -819,8 +879,12 @@ void trtri_impl(cudaStream_t st, int n, const double2* A, int lda, const Chol& c
     Q3B_CUDA(cudaMemsetAsync(Ui, 0, (size_t)n * n * sizeof(double2), st));
     trtri_diag<<<nblk, 256, 0, st>>>(n, c.dinv, Ui);
     Q3B_LAUNCH_CHECK();
-    for (int j = 1; j < nblk; ++j) {
-        trtri_col<<<j, 256, 0, st>>>(n, j, A, lda, c.dinv, Ui);
+    for (int m = NB; m < n; m *= 2) {
+        const int pairs = ceil_div(n, 2 * m);
+        const dim3 grid(pairs, m / NB, m / NB);
+        trtri_level<<<grid, 256, 0, st>>>(n, m, 0, A, lda, Ui, c.tbuf);
+        Q3B_LAUNCH_CHECK();
+        trtri_level<<<grid, 256, 0, st>>>(n, m, 1, A, lda, Ui, c.tbuf);
         Q3B_LAUNCH_CHECK();
     }
 }
@@ -829,7 +893,7 @@ void trtri_impl(cudaStream_t st, int n, const double2* A, int lda, const Chol& c
 
 size_t potrf_scratch_bytes(int n) {
     const size_t nblk = (size_t)ceil_div(n, NB);
-    return nblk * NB * NB * sizeof(double2) + 1024;
+    return nblk * NB * NB * sizeof(double2) + trtri_tbuf_elems(n) * sizeof(double2) + 2048;
 }
 
 size_t hegv_scratch_bytes(int n) {
@@ -859,7 +923,7 @@ void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, S
     double* d = ws.take<double>(n);
     double2* e = ws.take<double2>(n);
     double2* W = ws.take<double2>((size_t)n * n);
-    double2* xbuf = ws.take<double2>(n);
+    double2* xpre = ws.take<double2>(2 * (size_t)n);
     double2* pbuf = ws.take<double2>(2 * (size_t)n);
     double* ea = ws.take<double>(n);
     double* e2 = ws.take<double>(n);
@@ -876,15 +940,14 @@ void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, S
     int G = std::max(1, std::min(nsm, (n + 7) / 8));
     int cpb = (n + G - 1) / G;
     const size_t limit = 200 * 1024;
-    size_t smem = ((size_t)cpb * n + 2 * (size_t)n) * sizeof(double2);
+    size_t smem = ((size_t)cpb * n + 3 * (size_t)n) * sizeof(double2);
     if (smem > limit) throw Status(Q3B_ERR_INVALID, "subspace of order " + std::to_string(n) + " too large for the eigensolver");
     int w_in_smem = (smem + (size_t)cpb * n * sizeof(double2) <= limit) ? 1 : 0;
     if (w_in_smem) smem += (size_t)cpb * n * sizeof(double2);
     double2* partial = ws.take<double2>(2 * (size_t)G);
-    unsigned* bar = ws.take<unsigned>(2 + (size_t)n);
-    unsigned* ready = bar + 2;
+    unsigned* bar = ws.take<unsigned>(2);
     int* err = ws.take<int>(1);
-    Q3B_CUDA(cudaMemsetAsync(bar, 0, (2 + (size_t)n) * sizeof(unsigned), st));
+    Q3B_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
     Q3B_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
     static std::once_flag once;
     std::call_once(once, [limit] {
@@ -894,7 +957,7 @@ void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, S
     Q3B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_smem, 256, smem));
     if (per_sm < 1 || per_sm * nsm < G) throw Status(Q3B_ERR_INVALID, "eigensolver blocks cannot be co-resident");
     const double2* Ac = A;
-    void* args[] = {&n, &cpb, &w_in_smem, &Ac, &d, &e, &W, &xbuf, &pbuf, &partial, &bar, &ready, &err};
+    void* args[] = {&n, &cpb, &w_in_smem, &Ac, &d, &e, &W, &xpre, &pbuf, &partial, &bar, &err};
     Q3B_CUDA(cudaLaunchCooperativeKernel((const void*)hetrd_smem, dim3(G), dim3(256), args, smem, st));
     Q3B_LAUNCH_CHECK();
     tridiag_prep<<<1, 32, 0, st>>>(n, d, e, ea, e2, phase, bounds);
