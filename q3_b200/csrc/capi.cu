@@ -1,3 +1,4 @@
+#include <algorithm>
 // extern "C" entry points of libq3b (include/q3b.h).  Every call converts
 // exceptions to a status code and keeps the message on the context.
 #include <chrono>
@@ -134,21 +135,50 @@ int q3b_apply_h_f32(q3b_context* ctx, const q3b_cplx64* psi, q3b_cplx64* hpsi, i
     });
 }
 
+// Host vectors in and out.  The bands go through in chunks on three streams:
+// chunk i's copy in, its application on the context's stream and its copy out
+// run while chunk i+1 is copied in and chunk i-1 copied out, so the two copy
+// directions and the kernels overlap.  Pinned host buffers make the copies
+// asynchronous; pageable ones still work, serialised by the driver.
 int q3b_apply_h_host(q3b_context* ctx, const q3b_cplx128* psi, q3b_cplx128* hpsi, int nvec,
                      int precision) {
     return guarded(ctx, [&](Context& c) {
         c.require_ready();
         if (nvec <= 0) return;
         if (!psi || !hpsi) throw q3b::Status(Q3B_ERR_INVALID, "bad vectors");
-        const size_t n = (size_t)c.kp.npw * nvec;
+        const int npw = c.kp.npw;
+        const size_t n = (size_t)npw * nvec;
         c.ws_host_io.reserve(&c, 2 * n * sizeof(double2));
         double2* din = c.ws_host_io.as<double2>();
         double2* dout = din + n;
-        Q3B_CUDA(cudaMemcpyAsync(din, psi, n * sizeof(double2), cudaMemcpyHostToDevice, c.stream));
-        int rc = q3b_apply_h(ctx, reinterpret_cast<q3b_cplx128*>(din), reinterpret_cast<q3b_cplx128*>(dout),
-                             nvec, precision);
-        if (rc != Q3B_OK) throw q3b::Status(rc, c.err);
-        Q3B_CUDA(cudaMemcpyAsync(hpsi, dout, n * sizeof(double2), cudaMemcpyDeviceToHost, c.stream));
+        c.ensure_io_streams();
+        const int nchunk = nvec >= 32 ? Context::kIoChunks : 1;
+        const int per = (nvec + nchunk - 1) / nchunk;
+        const auto* hin = reinterpret_cast<const double2*>(psi);
+        auto* hout = reinterpret_cast<double2*>(hpsi);
+        for (int i = 0; i < nchunk; ++i) {
+            const int b0 = i * per, nb = std::min(per, nvec - b0);
+            if (nb <= 0) break;
+            const size_t off = (size_t)b0 * npw, bytes = (size_t)nb * npw * sizeof(double2);
+            Q3B_CUDA(cudaMemcpyAsync(din + off, hin + off, bytes, cudaMemcpyHostToDevice, c.io_in));
+            Q3B_CUDA(cudaEventRecord(c.io_ev_in[i], c.io_in));
+        }
+        for (int i = 0; i < nchunk; ++i) {
+            const int b0 = i * per, nb = std::min(per, nvec - b0);
+            if (nb <= 0) break;
+            const size_t off = (size_t)b0 * npw, bytes = (size_t)nb * npw * sizeof(double2);
+            Q3B_CUDA(cudaStreamWaitEvent(c.stream, c.io_ev_in[i], 0));
+            const int rc = q3b_apply_h(ctx, reinterpret_cast<q3b_cplx128*>(din + off),
+                                       reinterpret_cast<q3b_cplx128*>(dout + off), nb, precision);
+            if (rc != Q3B_OK) {
+                cudaStreamSynchronize(c.io_in);
+                throw q3b::Status(rc, c.err);
+            }
+            Q3B_CUDA(cudaEventRecord(c.io_ev_out[i], c.stream));
+            Q3B_CUDA(cudaStreamWaitEvent(c.io_out, c.io_ev_out[i], 0));
+            Q3B_CUDA(cudaMemcpyAsync(hout + off, dout + off, bytes, cudaMemcpyDeviceToHost, c.io_out));
+        }
+        Q3B_CUDA(cudaStreamSynchronize(c.io_out));
         Q3B_CUDA(cudaStreamSynchronize(c.stream));
         q3b::tc::check_error(c.stream);
     });

@@ -31,7 +31,8 @@ cgemm_kernel(int M, int N, int K, cplx_t<R> alpha, const cplx_t<R>* __restrict__
 
     const int tid = threadIdx.x;
     const int tx = tid % 16, ty = tid / 16;
-    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    // N tiles run fastest: the blocks that share an A tile run together
+    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
     const int kbeg = blockIdx.z * kchunk;
     const int kend = min(K, kbeg + kchunk);
 
@@ -205,7 +206,8 @@ void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, cplx_t<R> alpha, c
         kchunk = ceil_div(kchunk, BK) * BK;
         splits = ceil_div(K, kchunk);
     }
-    dim3 grid(ceil_div(M, kBM), ceil_div(N, kBN), splits);
+    if (ceil_div(M, kBM) > 65535) throw std::runtime_error("complex GEMM: M too large");
+    dim3 grid(ceil_div(N, kBN), ceil_div(M, kBM), splits);
     T* part = splits > 1 ? static_cast<T*>(ws.ptr) : nullptr;
     if (conj_a)
         cgemm_kernel<R, true><<<grid, kThreads, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,

@@ -17,12 +17,15 @@
 //   P = Ar [Br | Bi]^T  and  Q = Ai [Br | Bi]^T   (x3 for the split terms)
 // into two FP32 accumulators of 128 TMEM columns, and the epilogue forms
 //   C,N: Re = P_r + Q_i,  Im = P_i - Q_r      N,N: Re = P_r - Q_i,  Im = P_i + Q_r.
-// Warps 0-3 load a K block with coalesced 16-byte loads (all issued before any
-// conversion), split and de-interleave it into the planes and signal a "full"
-// mbarrier; the MMA thread commits each stage to an "empty" mbarrier; two
-// stages.  After the last block warps 0-3 read the accumulators with
-// tcgen05.ld (one TMEM lane per output row) and write C, or the raw sums of
-// their K range for a fixed-order split-K reduction.  Every mbarrier wait is
+// Two producer groups of four warps each own one of the two stages: a group
+// loads a K block with coalesced 16-byte loads (all issued before any
+// conversion), splits and de-interleaves it into the planes and signals the
+// stage's "full" mbarrier, so one group converts while the other's loads are
+// in flight.  The MMA thread (warp 8) commits each stage to an "empty"
+// mbarrier.  After the last block all eight producer warps read the
+// accumulators with tcgen05.ld (warp w: TMEM lanes 32*(w%4).., column half
+// w/4) and write C, or the raw sums of their K range for a fixed-order
+// split-K reduction.  Every mbarrier wait is
 // bounded; a timeout sets an error word and the block drains and frees TMEM.
 #include <cstdint>
 #include <mutex>
@@ -37,8 +40,11 @@ constexpr int BM = 128;            // complex rows per block (UMMA M)
 constexpr int BN = 64;             // complex columns per block (UMMA N)
 constexpr int BK = 32;             // K per stage: one 128-byte TF32 row
 constexpr int STAGES = 2;
-constexpr int PRODUCERS = 128;     // warps 0-3
-constexpr int THREADS = PRODUCERS + 32;
+constexpr int PRODUCERS = 128;     // threads of one producer group (4 warps)
+constexpr int GROUPS = 2;          // producer groups: group g fills stage g
+constexpr int MMA_WARP = 4 * GROUPS;
+constexpr int THREADS = GROUPS * PRODUCERS + 32;
+static_assert(GROUPS == STAGES, "each producer group owns one stage");
 constexpr int A_PLANE = BM * 128;      // bytes of one A plane (BM rows x 128 B)
 constexpr int B_PLANE = 2 * BN * 128;  // bytes of one B plane (re rows + im rows)
 constexpr int UMMA_N = 2 * BN;         // [Br | Bi]
@@ -309,7 +315,9 @@ cgemm_tc_kernel(int M, int N, int K, float2 alpha, const float2* __restrict__ A,
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    // N tiles run fastest, so the blocks that share an A tile run together and
+    // all but the first find it in L2
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int kbeg = blockIdx.z * kchunk;
     const int kend = min(K, kbeg + kchunk);
     const int nkb = kend > kbeg ? (kend - kbeg + BK - 1) / BK : 0;
@@ -334,9 +342,13 @@ cgemm_tc_kernel(int M, int N, int K, float2 alpha, const float2* __restrict__ A,
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
 
-    if (warp < 4) {
+    if (warp < MMA_WARP) {
         // ---------------------------------------------------------- producers
-        for (int kb = 0; kb < nkb; ++kb) {
+        // group g loads K blocks g, g + GROUPS, ... into stage g: while one
+        // group waits on its loads the other converts, so two K blocks are
+        // in flight
+        const int g = warp / 4, ptid = tid % PRODUCERS;
+        for (int kb = g; kb < nkb; kb += GROUPS) {
             const int s = kb % STAGES;
             if (kb >= STAGES && !mbar_wait(&empty_bar[s], ((kb / STAGES) - 1) & 1, err)) break;
             unsigned char* st = smem + s * STAGE_BYTES;
@@ -344,15 +356,15 @@ cgemm_tc_kernel(int M, int N, int K, float2 alpha, const float2* __restrict__ A,
             unsigned char* pb = st + 4 * A_PLANE;
             const int k0 = kbeg + kb * BK;
             if (CONJ_A)
-                load_kmajor<BM>(pa, A_PLANE, A, lda, m0, M, k0, kend, tid);
+                load_kmajor<BM>(pa, A_PLANE, A, lda, m0, M, k0, kend, ptid);
             else
-                load_mmajor(pa, A_PLANE, A, lda, m0, M, k0, kend, tid);
-            load_b(pb, B, ldb, n0, N, k0, kend, tid);
+                load_mmajor(pa, A_PLANE, A, lda, m0, M, k0, kend, ptid);
+            load_b(pb, B, ldb, n0, N, k0, kend, ptid);
             fence_async_smem();
             mbar_arrive(&full_bar[s]);
         }
     } else if (lane == 0) {
-        // ------------------------------------------------------- MMA issuer
+        // ------------------------------------------------------- MMA issuer (warp MMA_WARP)
         // per K step: P += Ar [Br|Bi]^T, Q += Ai [Br|Bi]^T, each as hi*hi + hi*lo + lo*hi
         bool first = true;
         bool ok = true;
@@ -387,15 +399,17 @@ cgemm_tc_kernel(int M, int N, int K, float2 alpha, const float2* __restrict__ A,
     }
 
     // ------------------------------------------------------------ epilogue
-    if (warp < 4) {
+    // warp w reads TMEM lanes 32*(w%4).. (its rows) for columns half w/4
+    if (warp < MMA_WARP) {
         const bool waited = nkb > 0 && mbar_wait(&done_bar, 0, err);
         const bool have = __all_sync(0xffffffffu, waited);  // tcgen05.ld is warp-collective
         tc_fence_after();
-        const int row = m0 + warp * 32 + lane;
-        const uint32_t lane_addr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+        const int q = warp & 3, h = warp >> 2;
+        const int row = m0 + q * 32 + lane;
+        const uint32_t lane_addr = tmem + (static_cast<uint32_t>(q * 32) << 16);
         const bool use_beta = (beta.x != 0.f || beta.y != 0.f);
 #pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 16) {
+        for (int c0 = h * (BN / GROUPS); c0 < (h + 1) * (BN / GROUPS); c0 += 16) {
             float pr[16], pi[16], qr[16], qi[16];
             if (have) {
                 tmem_ld16(lane_addr + c0, pr);                  // Ar Br
@@ -522,7 +536,8 @@ void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, cons
         kchunk = ceil_div(ceil_div(K, splits), BK) * BK;
         splits = ceil_div(K, kchunk);
     }
-    dim3 grid(ceil_div(M, BM), ceil_div(N, BN), splits);
+    if (ceil_div(M, BM) > 65535) throw std::runtime_error("tensor-core GEMM: M too large");
+    dim3 grid(ceil_div(N, BN), ceil_div(M, BM), splits);
     float2* part = splits > 1 ? static_cast<float2*>(ws.ptr) : nullptr;
     if (conj_a)
         cgemm_tc_kernel<true><<<grid, THREADS, SMEM_BYTES, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,

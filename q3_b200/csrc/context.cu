@@ -62,6 +62,26 @@ Context::~Context() {
     cudaSetDevice(device);
     cudaStreamSynchronize(stream);
     if (own_stream) cudaStreamDestroy(own_stream);
+    if (io_in) {
+        cudaStreamSynchronize(io_in);
+        cudaStreamSynchronize(io_out);
+        for (int i = 0; i < kIoChunks; ++i) {
+            cudaEventDestroy(io_ev_in[i]);
+            cudaEventDestroy(io_ev_out[i]);
+        }
+        cudaStreamDestroy(io_in);
+        cudaStreamDestroy(io_out);
+    }
+}
+
+void Context::ensure_io_streams() {
+    if (io_in) return;
+    Q3B_CUDA(cudaStreamCreateWithFlags(&io_in, cudaStreamNonBlocking));
+    Q3B_CUDA(cudaStreamCreateWithFlags(&io_out, cudaStreamNonBlocking));
+    for (int i = 0; i < kIoChunks; ++i) {
+        Q3B_CUDA(cudaEventCreateWithFlags(&io_ev_in[i], cudaEventDisableTiming));
+        Q3B_CUDA(cudaEventCreateWithFlags(&io_ev_out[i], cudaEventDisableTiming));
+    }
 }
 
 GemmWorkspace Context::gemm_ws(size_t need) {

@@ -79,6 +79,12 @@ class Context {
     int start_n = 0;
     int start_npw = 0;
 
+    // copy streams and events of q3b_apply_h_host's pipelined chunks
+    static constexpr int kIoChunks = 4;
+    cudaStream_t io_in = nullptr, io_out = nullptr;
+    cudaEvent_t io_ev_in[kIoChunks] = {}, io_ev_out[kIoChunks] = {};
+    void ensure_io_streams();
+
     explicit Context(int dev, size_t hbm_budget);
     ~Context();
 

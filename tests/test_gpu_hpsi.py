@@ -126,3 +126,18 @@ def test_hpsi_empty_batch_and_errors(cuda_device):
     ap.apply_batch(y, y.clone(), 0)        # empty batch is a no-op
     with pytest.raises(Q3BError):          # unsupported grid length (7)
         ap.update_potential(np.zeros(7 * 8 * 8), (7, 8, 8))
+
+
+@pytest.mark.parametrize("nvec", [8, 37, 64])
+def test_host_buffer_path_matches_device_path(cuda_device, nvec):
+    """q3b_apply_h_host (host vectors, chunked copy/compute pipeline for
+    32 bands and more) against q3b_apply_h on device vectors."""
+    sy = synthetic.small_system(grid=(16, 16, 16), a=8.0, ecut=12.0, nbands=nvec, natoms=3, seed=5)
+    ap = _applicator(sy)
+    psi = sy.psi0[0][:, :nvec]
+    for prec, tol in ((FP64, 1e-13), (MIXED, 1e-6)):
+        dev = _run(ap, psi, prec)
+        host = ap.apply_batch_host(psi, nvec, prec)
+        assert _rel(host, dev) < tol
+    ref = ohpsi.apply_h(psi, sy.kpoints[0], sy.v_r, sy.cell.grid)
+    assert _rel(ap.apply_batch_host(psi, nvec, FP64), ref) < FP64_TOL
