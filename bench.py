@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=32)
     ap.add_argument("--serving-rate", type=float, default=0.0,
                     help="arrivals per second (default: 80%% of the measured FP64 capacity)")
+    ap.add_argument("--probe", choices=["mixed", "fp64"], default=None,
+                    help="profiling aid: apply H to the bench block three times in one precision "
+                         "(after the plane-kernel tuning) and exit; prints no bench line")
     return ap.parse_args()
 
 
@@ -513,8 +516,31 @@ def run_q3b(args):
         pg.destroy_process_group()
 
 
+def run_probe(args):
+    """Three H|psi> applications of the bench block in one precision: a short,
+    fixed launch sequence for ncu captures of the plane and GEMM kernels."""
+    import torch
+    from q3_b200 import synthetic
+    from q3_b200._lib import FP64, MIXED
+    from q3_b200.applicator import PlanewaveHamiltonianApplicator
+    sy = synthetic.config(1)
+    ap = PlanewaveHamiltonianApplicator()
+    ap.update_potential(sy.v_r, sy.cell.grid)
+    ap.prepare_system_kpoint(sy)
+    x = torch.from_numpy(np.ascontiguousarray(sy.psi0[0].T)).to("cuda")
+    y = torch.empty_like(x)
+    prec = MIXED if args.probe == "mixed" else FP64
+    for _ in range(3):
+        ap.apply_batch(x, y, sy.nbands, prec)
+    torch.cuda.synchronize()
+    print(json.dumps({"probe": args.probe, "norm": float(torch.linalg.norm(y).item())}), flush=True)
+
+
 def main():
     args = parse()
+    if args.probe:
+        run_probe(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

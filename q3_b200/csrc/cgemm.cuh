@@ -32,6 +32,23 @@ template <typename R> size_t cgemm_workspace_bytes(int M, int N, int K);
 namespace tc {
 void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, const float2* A, long lda,
            const float2* B, long ldb, float2 beta, float2* C, long ldc, const GemmWorkspace& ws);
+
+// An A operand converted once into the shared-memory image the tensor-core
+// kernel's stages take (TF32 hi/lo planes, 128B-swizzled, tiles of 128 rows x
+// 32 K), for operands used many times, such as a k-point's projectors: the
+// kernel then moves its A tiles with bulk asynchronous copies and converts
+// only B.  Rows are M of the product, K its reduction index.
+struct PackedA {
+    const unsigned char* tiles = nullptr;
+    int M = 0, K = 0;
+};
+size_t packed_a_bytes(int M, int K);
+// kmajor: element (m, k) at A[m * lda + k] (the "C,N" operand, A^H's source);
+// else at A[m + k * lda] (the "N,N" operand).  out: packed_a_bytes(M, K).
+void pack_a(cudaStream_t st, int M, int K, const float2* A, long lda, bool kmajor, unsigned char* out);
+// cgemm with a packed A (same meaning of conj_a and the other arguments)
+void cgemm_packed(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, const PackedA& A,
+                  const float2* B, long ldb, float2 beta, float2* C, long ldc, const GemmWorkspace& ws);
 size_t workspace_bytes(int M, int N, int K);
 // device word the tensor-core kernels set when a pipeline wait times out
 int* error_word();

@@ -86,6 +86,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
 }
 
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// raise the transaction count the barrier's current phase waits for
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// bulk asynchronous copy global -> this block's shared memory, completing
+// `bytes` of the barrier's transaction count (16-byte aligned, size % 16 == 0)
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -300,11 +314,42 @@ __device__ __forceinline__ void load_b(unsigned char* planes, const float2* X, l
     }
 }
 
-template <bool CONJ_A>
+// One packed A tile (128 rows x 32 K, four 16 KB planes) per block: built in
+// shared memory, then written out contiguously.  Tiles are stored K-block
+// fastest: tile (mt, kb) at (mt * nkt + kb) * A_TILE bytes.
+constexpr int A_TILE = 4 * A_PLANE;
+__global__ void __launch_bounds__(256)
+pack_a_kernel(int M, int K, const float2* __restrict__ A, long lda, int kmajor, int nkt, unsigned char* out) {
+    extern __shared__ __align__(1024) unsigned char tile[];
+    const int mt = blockIdx.x / nkt, kb = blockIdx.x % nkt;
+    for (int idx = threadIdx.x; idx < BM * BK; idx += blockDim.x) {
+        // lanes along the operand's contiguous index, for coalesced reads
+        const int r = kmajor ? idx / BK : idx % BM;
+        const int k = kmajor ? idx % BK : idx / BM;
+        const int gm = mt * BM + r, gk = kb * BK + k;
+        float2 x = make_float2(0.f, 0.f);
+        if (gm < M && gk < K) x = kmajor ? A[(long)gm * lda + gk] : A[gm + (long)gk * lda];
+        const float rh = tf32_rn(x.x), ih = tf32_rn(x.y);
+        const uint32_t o = swz(r, k);
+        *reinterpret_cast<float*>(tile + 0 * A_PLANE + o) = rh;
+        *reinterpret_cast<float*>(tile + 1 * A_PLANE + o) = tf32_rn(x.x - rh);
+        *reinterpret_cast<float*>(tile + 2 * A_PLANE + o) = ih;
+        *reinterpret_cast<float*>(tile + 3 * A_PLANE + o) = tf32_rn(x.y - ih);
+    }
+    __syncthreads();
+    float4* dst = reinterpret_cast<float4*>(out + (size_t)blockIdx.x * A_TILE);
+    const float4* src = reinterpret_cast<const float4*>(tile);
+    for (int i = threadIdx.x; i < A_TILE / 16; i += blockDim.x) dst[i] = src[i];
+}
+
+// PACKED_A: A's tiles come from a pack_a_kernel image by bulk copies (one
+// thread of the stage's producer group issues them), and the group converts
+// only B; the stage's barrier waits for the copies' bytes as well.
+template <bool CONJ_A, bool PACKED_A>
 __global__ void __launch_bounds__(THREADS, 1)
 cgemm_tc_kernel(int M, int N, int K, float2 alpha, const float2* __restrict__ A, long lda,
-                const float2* __restrict__ B, long ldb, float2 beta, float2* C, long ldc, int kchunk,
-                float2* part, int* err) {
+                const unsigned char* __restrict__ Apk, const float2* __restrict__ B, long ldb, float2 beta,
+                float2* C, long ldc, int kchunk, float2* part, int* err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[STAGES];
     __shared__ __align__(8) uint64_t empty_bar[STAGES];
@@ -355,10 +400,20 @@ cgemm_tc_kernel(int M, int N, int K, float2 alpha, const float2* __restrict__ A,
             unsigned char* pa = st;
             unsigned char* pb = st + 4 * A_PLANE;
             const int k0 = kbeg + kb * BK;
-            if (CONJ_A)
+            if (PACKED_A) {
+                if (ptid == 0) {
+                    const int nkt = (K + BK - 1) / BK;
+                    const unsigned char* src = Apk + ((size_t)blockIdx.y * nkt + k0 / BK) * A_TILE;
+                    mbar_expect_tx(&full_bar[s], A_TILE);
+#pragma unroll
+                    for (int pl = 0; pl < 4; ++pl)
+                        bulk_copy_g2s(pa + pl * A_PLANE, src + pl * A_PLANE, A_PLANE, &full_bar[s]);
+                }
+            } else if (CONJ_A) {
                 load_kmajor<BM>(pa, A_PLANE, A, lda, m0, M, k0, kend, ptid);
-            else
+            } else {
                 load_mmajor(pa, A_PLANE, A, lda, m0, M, k0, kend, ptid);
+            }
             load_b(pb, B, ldb, n0, N, k0, kend, ptid);
             fence_async_smem();
             mbar_arrive(&full_bar[s]);
@@ -520,13 +575,23 @@ size_t workspace_bytes(int M, int N, int K) {
     return s > 1 ? (size_t)s * M * N * sizeof(float2) : 0;
 }
 
-void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, const float2* A, long lda,
-           const float2* B, long ldb, float2 beta, float2* C, long ldc, const GemmWorkspace& ws) {
+namespace {
+
+template <bool CONJ_A, bool PACKED_A> void set_kernel_smem() {
+    cudaFuncSetAttribute(cgemm_tc_kernel<CONJ_A, PACKED_A>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+}
+
+void launch(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, const float2* A, long lda,
+            const unsigned char* Apk, const float2* B, long ldb, float2 beta, float2* C, long ldc,
+            const GemmWorkspace& ws) {
     int* err = error_word();
     static std::once_flag once;
     std::call_once(once, [] {
-        cudaFuncSetAttribute(cgemm_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-        cudaFuncSetAttribute(cgemm_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+        set_kernel_smem<true, false>();
+        set_kernel_smem<false, false>();
+        set_kernel_smem<true, true>();
+        set_kernel_smem<false, true>();
+        cudaFuncSetAttribute(pack_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, A_TILE);
     });
     int splits = conj_a ? choose_splits(M, N, K) : 1;
     const size_t need = (size_t)splits * M * N * sizeof(float2);
@@ -539,12 +604,17 @@ void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, cons
     if (ceil_div(M, BM) > 65535) throw std::runtime_error("tensor-core GEMM: M too large");
     dim3 grid(ceil_div(N, BN), ceil_div(M, BM), splits);
     float2* part = splits > 1 ? static_cast<float2*>(ws.ptr) : nullptr;
-    if (conj_a)
-        cgemm_tc_kernel<true><<<grid, THREADS, SMEM_BYTES, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
-                                                                 kchunk, part, err);
-    else
-        cgemm_tc_kernel<false><<<grid, THREADS, SMEM_BYTES, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
-                                                                  kchunk, part, err);
+#define Q3B_TC_LAUNCH(CA, PA)                                                                             \
+    cgemm_tc_kernel<CA, PA><<<grid, THREADS, SMEM_BYTES, st>>>(M, N, K, alpha, A, lda, Apk, B, ldb, beta, C, \
+                                                               ldc, kchunk, part, err)
+    if (Apk) {
+        if (conj_a) Q3B_TC_LAUNCH(true, true);
+        else Q3B_TC_LAUNCH(false, true);
+    } else {
+        if (conj_a) Q3B_TC_LAUNCH(true, false);
+        else Q3B_TC_LAUNCH(false, false);
+    }
+#undef Q3B_TC_LAUNCH
     Q3B_LAUNCH_CHECK();
     if (splits > 1) {
         const long total = (long)M * N;
@@ -553,6 +623,36 @@ void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, cons
         splitk_sum<<<blocks, 256, 0, st>>>(M, N, splits, part, alpha, beta, C, ldc);
         Q3B_LAUNCH_CHECK();
     }
+}
+
+}  // namespace
+
+void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, const float2* A, long lda,
+           const float2* B, long ldb, float2 beta, float2* C, long ldc, const GemmWorkspace& ws) {
+    launch(st, conj_a, M, N, K, alpha, A, lda, nullptr, B, ldb, beta, C, ldc, ws);
+}
+
+size_t packed_a_bytes(int M, int K) {
+    return (size_t)ceil_div(M, BM) * ceil_div(K, BK) * A_TILE;
+}
+
+void pack_a(cudaStream_t st, int M, int K, const float2* A, long lda, bool kmajor, unsigned char* out) {
+    if (M <= 0 || K <= 0) return;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaFuncSetAttribute(pack_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, A_TILE);
+    });
+    const int nkt = ceil_div(K, BK);
+    const long tiles = (long)ceil_div(M, BM) * nkt;
+    if (tiles > 0x7fffffffL) throw std::runtime_error("tensor-core GEMM: operand too large to pack");
+    pack_a_kernel<<<static_cast<unsigned>(tiles), 256, A_TILE, st>>>(M, K, A, lda, kmajor ? 1 : 0, nkt, out);
+    Q3B_LAUNCH_CHECK();
+}
+
+void cgemm_packed(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, const PackedA& A,
+                  const float2* B, long ldb, float2 beta, float2* C, long ldc, const GemmWorkspace& ws) {
+    if (!A.tiles || A.M != M || A.K != K) throw std::runtime_error("tensor-core GEMM: packed A of another shape");
+    launch(st, conj_a, M, N, K, alpha, nullptr, 0, A.tiles, B, ldb, beta, C, ldc, ws);
 }
 
 }  // namespace tc

@@ -305,6 +305,10 @@ void Context::prepare_kpoint(int npw, const int32_t* g2g, const double* ke, cons
         std::vector<float2> b32(nb);
         for (size_t i = 0; i < nb; ++i) b32[i] = make_float2((float)beta[i].x, (float)beta[i].y);
         upload(this, kp.beta32, b32.data(), nb);
+        kp.beta_pk_overlap.reserve(this, tc::packed_a_bytes(nproj, npw));
+        kp.beta_pk_accum.reserve(this, tc::packed_a_bytes(npw, nproj));
+        tc::pack_a(stream, nproj, npw, kp.beta32.as<float2>(), npw, true, kp.beta_pk_overlap.as<unsigned char>());
+        tc::pack_a(stream, npw, nproj, kp.beta32.as<float2>(), npw, false, kp.beta_pk_accum.as<unsigned char>());
         std::vector<int> ps(nproj), pz(nproj), po(nproj);
         std::vector<double> d64;
         size_t doff = 0;
@@ -341,8 +345,13 @@ template <> NonlocalData<double> Context::nonlocal<double>() const {
                                 kp.psize.as<int>(), kp.poff.as<int>(), kp.dpk64.as<double>()};
 }
 template <> NonlocalData<float> Context::nonlocal<float>() const {
-    return NonlocalData<float>{kp.nproj, kp.beta32.as<float2>(), kp.pstart.as<int>(),
-                               kp.psize.as<int>(), kp.poff.as<int>(), kp.dpk32.as<float>()};
+    NonlocalData<float> d{kp.nproj, kp.beta32.as<float2>(), kp.pstart.as<int>(),
+                          kp.psize.as<int>(), kp.poff.as<int>(), kp.dpk32.as<float>()};
+    if (kp.nproj > 0) {
+        d.beta_overlap = tc::PackedA{kp.beta_pk_overlap.as<unsigned char>(), kp.nproj, kp.npw};
+        d.beta_accum = tc::PackedA{kp.beta_pk_accum.as<unsigned char>(), kp.npw, kp.nproj};
+    }
+    return d;
 }
 
 template <typename R> int Context::sticks_chunk(int nvec) const {

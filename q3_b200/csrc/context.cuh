@@ -46,6 +46,7 @@ struct KPoint {
     std::vector<double> ke_host;
     DevBuf ke64, ke32;
     DevBuf beta64, beta32;
+    DevBuf beta_pk_overlap, beta_pk_accum;  // beta32 as packed tensor-core A tiles
     DevBuf pstart, psize, poff, dpk64, dpk32;
     // sticks plan
     DevBuf stick_start, entry_g, entry_w3, entry_stick, stick_pos, row_base, unmapped;

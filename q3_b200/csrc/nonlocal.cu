@@ -1,3 +1,4 @@
+#include <type_traits>
 // Kleinman-Bylander term and small elementwise helpers.
 //
 // hpsi += beta D beta^H psi, as SerialPlanewaveHamiltonianApplicator does it
@@ -59,7 +60,14 @@ void apply_nonlocal(cudaStream_t st, const NonlocalData<R>& nl, int npw, int nve
     if (nl.nproj <= 0 || nvec <= 0) return;
     const T one = mk(R(1), R(0)), zero = mk(R(0), R(0));
     if (tm) tm->begin(PhaseTimer::PROJ_OVERLAP);
-    cgemm<R>(st, true, nl.nproj, nvec, npw, one, nl.beta, npw, psi, ldpsi, zero, Bm, nl.nproj, ws);
+    if constexpr (std::is_same<R, float>::value) {
+        if (nl.beta_overlap.tiles)
+            tc::cgemm_packed(st, true, nl.nproj, nvec, npw, one, nl.beta_overlap, psi, ldpsi, zero, Bm, nl.nproj, ws);
+        else
+            cgemm<R>(st, true, nl.nproj, nvec, npw, one, nl.beta, npw, psi, ldpsi, zero, Bm, nl.nproj, ws);
+    } else {
+        cgemm<R>(st, true, nl.nproj, nvec, npw, one, nl.beta, npw, psi, ldpsi, zero, Bm, nl.nproj, ws);
+    }
     if (tm) tm->end();
     if (tm) tm->begin(PhaseTimer::D_APPLY);
     apply_d_blocks<R><<<grid_for((long)nl.nproj * nvec), 256, 0, st>>>(
@@ -67,7 +75,14 @@ void apply_nonlocal(cudaStream_t st, const NonlocalData<R>& nl, int npw, int nve
     Q3B_LAUNCH_CHECK();
     if (tm) tm->end();
     if (tm) tm->begin(PhaseTimer::PROJ_ACCUM);
-    cgemm<R>(st, false, npw, nvec, nl.nproj, one, nl.beta, npw, Bp, nl.nproj, one, hpsi, ldh, ws);
+    if constexpr (std::is_same<R, float>::value) {
+        if (nl.beta_accum.tiles)
+            tc::cgemm_packed(st, false, npw, nvec, nl.nproj, one, nl.beta_accum, Bp, nl.nproj, one, hpsi, ldh, ws);
+        else
+            cgemm<R>(st, false, npw, nvec, nl.nproj, one, nl.beta, npw, Bp, nl.nproj, one, hpsi, ldh, ws);
+    } else {
+        cgemm<R>(st, false, npw, nvec, nl.nproj, one, nl.beta, npw, Bp, nl.nproj, one, hpsi, ldh, ws);
+    }
     if (tm) tm->end();
 }
 

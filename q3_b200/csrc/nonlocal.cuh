@@ -14,6 +14,9 @@ template <typename R> struct NonlocalData {
     const int* psize = nullptr;       // size of p's atom block
     const int* poff = nullptr;        // offset of p's block in dpk
     const R* dpk = nullptr;           // packed column-major D blocks (Ry)
+    // FP32 only: beta pre-split into the tensor-core kernel's A tiles, for
+    // beta^H psi (rows = projectors) and for beta B' (rows = plane waves)
+    tc::PackedA beta_overlap{}, beta_accum{};
 };
 
 // hpsi += beta D beta^H psi.  Bm, Bp: nproj x nvec scratch each.

@@ -59,7 +59,8 @@ size_t estimate_bytes(const Job& j) {
     b += 10 * maxn * maxn * sizeof(double2) + dense::hegv_scratch_bytes((int)maxn) +
          dense::potrf_scratch_bytes((int)maxn);
     b += std::min<size_t>(48ull << 20, (size_t)j.nb * j.n3 * (size_t)j.n1 * j.n2 / 4 * sizeof(double2));
-    b += (size_t)j.npw * j.nproj * (sizeof(double2) + sizeof(float2));
+    // projectors: FP64, FP32 and the two packed tensor-core copies (16 B each)
+    b += (size_t)j.npw * j.nproj * (sizeof(double2) + sizeof(float2) + 32);
     b += N * (sizeof(double) + sizeof(float));
     b += 2 * (size_t)j.nproj * j.nb * sizeof(double2) + (16ull << 20);
     return b + b / 5;
