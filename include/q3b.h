@@ -260,6 +260,20 @@ int q3b_server_wait(q3b_server* server, int id, q3b_cplx128* bands_out, double* 
 int q3b_hegv(q3b_context* ctx, int n, const q3b_cplx128* h_dev, const q3b_cplx128* s_dev, int ld,
              double* w_dev, q3b_cplx128* evec_dev);
 
+/* ---- charge density (PlanewaveChargeDensityAccumulator) --------------------- */
+
+/* accumulate_on_rho_grid, non-Gamma branch
+ * (charge_density/planewave/internal/accumulator.hpp:375-545), for the context's
+ * prepared k-point on its grid: rho[(w1*N2 + w2)*N3 + w3] +=
+ * sum_b weights[b] |psi_b(r)|^2, psi_b(r) the unnormalised backward transform
+ * of band b (npw x nvec device vectors, FP64) scattered by the G -> grid map.
+ * weights (host, nvec) fold the k-point weight, the occupation and 1/volume;
+ * a band of weight 0 is skipped, as the reference skips unoccupied bands.
+ * rho: N1*N2*N3 doubles on the device, added to, so that k-points accumulate.
+ * Deterministic: the band sums have a fixed order. */
+int q3b_accumulate_density(q3b_context* ctx, const q3b_cplx128* psi_dev, int nvec, const double* weights_host,
+                           double* rho_dev);
+
 /* ---- starting-subspace rotation (StartingSubspaceSolver) -------------------- */
 
 /* The three large steps of the starting rotation of one k-point's bands

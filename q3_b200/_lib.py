@@ -106,6 +106,7 @@ SIGNATURES = {
     "q3b_davidson_solve_dev": (_i, [_vp, _vp, _vp, _i, C.POINTER(DavidsonOpts),
                                     C.POINTER(DavidsonStats)]),
     "q3b_hegv": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp]),
+    "q3b_accumulate_density": (_i, [_vp, _vp, _i, _vp, _vp]),
     "q3b_start_apply": (_i, [_vp, _vp, _i]),
     "q3b_start_project": (_i, [_vp, _vp, _vp]),
     "q3b_start_rotate": (_i, [_vp, _vp, _i, _vp]),

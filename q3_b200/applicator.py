@@ -141,6 +141,16 @@ class PlanewaveHamiltonianApplicator:
             raise ValueError("vectors must be complex128 (or complex64 for the FP32 entry)")
         check(self.h, rc)
 
+    def accumulate_density(self, bands, weights: np.ndarray, rho) -> None:
+        """PlanewaveChargeDensityAccumulator at this k-point: rho += sum_b w_b |psi_b(r)|^2.
+
+        bands: complex128 CUDA tensor nb x npw (band-contiguous); weights: nb
+        (k-point weight x occupation / cell volume; 0 skips a band); rho: float64
+        CUDA tensor of N1*N2*N3 values, natural grid order, added to."""
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        check(self.h, self.lib.q3b_accumulate_density(self.h, bands.data_ptr(), int(w.size), _ptr(w),
+                                                      rho.data_ptr()))
+
     def apply_batch_host(self, psi: np.ndarray, number_of_vectors: int,
                          precision: int = FP64) -> np.ndarray:
         x = np.asfortranarray(psi, dtype=np.complex128)

@@ -137,17 +137,16 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
+// 16 consecutive TMEM columns of this warp's 32 lanes; the values are valid
+// after tmem_wait_ld (several loads may be in flight before one wait)
+__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t* r) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ float tf32_rn(float x) {
     uint32_t r;
@@ -467,15 +466,34 @@ cgemm_tc_kernel(int M, int N, int K, float2 alpha, const float2* __restrict__ A,
         for (int c0 = h * (BN / GROUPS); c0 < (h + 1) * (BN / GROUPS); c0 += 16) {
             float pr[16], pi[16], qr[16], qi[16];
             if (have) {
-                tmem_ld16(lane_addr + c0, pr);                  // Ar Br
-                tmem_ld16(lane_addr + BN + c0, pi);             // Ar Bi
-                tmem_ld16(lane_addr + UMMA_N + c0, qr);         // Ai Br
-                tmem_ld16(lane_addr + UMMA_N + BN + c0, qi);    // Ai Bi
+                uint32_t r0[16], r1[16], r2[16], r3[16];
+                tmem_ld16_issue(lane_addr + c0, r0);                  // Ar Br
+                tmem_ld16_issue(lane_addr + BN + c0, r1);             // Ar Bi
+                tmem_ld16_issue(lane_addr + UMMA_N + c0, r2);         // Ai Br
+                tmem_ld16_issue(lane_addr + UMMA_N + BN + c0, r3);    // Ai Bi
+                tmem_wait_ld();
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    pr[j] = __uint_as_float(r0[j]);
+                    pi[j] = __uint_as_float(r1[j]);
+                    qr[j] = __uint_as_float(r2[j]);
+                    qi[j] = __uint_as_float(r3[j]);
+                }
             } else {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) pr[j] = pi[j] = qr[j] = qi[j] = 0.f;
             }
             if (row < M) {
+                // the 16 old values of C are read before any is written, so
+                // their latencies overlap
+                float2 old[16];
+                if (use_beta && !part) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int col = n0 + c0 + j;
+                        old[j] = col < N ? C[row + (long)col * ldc] : make_float2(0.f, 0.f);
+                    }
+                }
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     const int col = n0 + c0 + j;
@@ -486,13 +504,12 @@ cgemm_tc_kernel(int M, int N, int K, float2 alpha, const float2* __restrict__ A,
                         part[(long)blockIdx.z * M * N + (long)col * M + row] = acc;
                     } else {
                         float2 v = make_float2(alpha.x * acc.x - alpha.y * acc.y, alpha.x * acc.y + alpha.y * acc.x);
-                        float2* cp = C + row + (long)col * ldc;
                         if (use_beta) {
-                            const float2 o = *cp;
+                            const float2 o = old[j];
                             v.x += beta.x * o.x - beta.y * o.y;
                             v.y += beta.x * o.y + beta.y * o.x;
                         }
-                        *cp = v;
+                        C[row + (long)col * ldc] = v;
                     }
                 }
             }

@@ -388,7 +388,8 @@ template <typename R> void Context::tune_local() {
             return;
         }
     }
-    const int nb = 16;
+    // enough bands for a few planes per SM, as in a real application
+    const int nb = 64;
     const size_t n = (size_t)kp.npw * nb;
     ws_tune.reserve(this, 2 * n * sizeof(T));
     T* tin = ws_tune.as<T>();

@@ -75,6 +75,8 @@ class Context {
     // workspaces
     DevBuf ws_sticks, ws_gemm, ws_bm, ws_bp, ws_conv_in, ws_conv_out, ws_host_io;
     DevBuf ws_solver, ws_dense, ws_bands, ws_tune;
+    // charge density: per-group partial sums and the band weights
+    DevBuf ws_density;
     // starting-subspace rotation: chi and H chi of the last q3b_start_apply
     DevBuf ws_start;
     int start_n = 0;

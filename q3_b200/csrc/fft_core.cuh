@@ -154,8 +154,25 @@ __device__ __forceinline__ int digit_reversed(int pos, int na, int nb) { return 
 // write of every element with no hazard between items, and passes are
 // separated by one barrier.  Lines run fastest across lanes: the callers lay
 // lines out at an odd pitch, so a warp's accesses fall in distinct banks.
-template <int R, bool CONTIG, typename T, typename Body>
-__device__ __forceinline__ void line_pass(T* buf, const LineGeom& g, const Body& body) {
+// Which values of an item a pass reads and writes.  AllPositions: every
+// one.  ItemMask (stride-nb passes, CONTIG = false): bits[q] has bit r set
+// when position q + nb*r of the line holds data; a clear bit reads as zero on
+// load, or is not stored.  One shared-memory word per item, then register
+// bit tests.
+struct AllPositions {
+    static constexpr bool kAll = true;
+    __device__ __forceinline__ unsigned word(int) const { return ~0u; }
+};
+struct ItemMask {
+    static constexpr bool kAll = false;
+    const unsigned* bits;
+    __device__ __forceinline__ unsigned word(int q) const { return bits[q]; }
+};
+
+template <int R, bool CONTIG, typename T, typename Body, typename LoadSel = AllPositions,
+          typename StoreSel = AllPositions>
+__device__ __forceinline__ void line_pass(T* buf, const LineGeom& g, const Body& body, const LoadSel& lsel = {},
+                                          const StoreSel& ssel = {}) {
     const int Q = CONTIG ? g.na : g.nb;
     const int qs = (CONTIG ? g.nb : 1) * g.es;
     const int rs = (CONTIG ? 1 : g.nb) * g.es;
@@ -165,11 +182,16 @@ __device__ __forceinline__ void line_pass(T* buf, const LineGeom& g, const Body&
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
         T* p = buf + g.base(l) + q * qs;
         T x[R];
+        const unsigned lw = lsel.word(q), sw = ssel.word(q);
 #pragma unroll
-        for (int r = 0; r < R; ++r) x[r] = p[r * rs];
+        for (int r = 0; r < R; ++r) {
+            if (LoadSel::kAll || ((lw >> r) & 1u)) x[r] = p[r * rs];
+            else x[r] = czero<T>();
+        }
         body(x, l, q);
 #pragma unroll
-        for (int r = 0; r < R; ++r) p[r * rs] = x[r];
+        for (int r = 0; r < R; ++r)
+            if (StoreSel::kAll || ((sw >> r) & 1u)) p[r * rs] = x[r];
         l += br;
         q += bq;
         if (l >= g.lines) {
@@ -195,8 +217,9 @@ __device__ __forceinline__ void line_pass(T* buf, const LineGeom& g, const Body&
 // A backward-then-forward round trip fuses B+ and B- in registers, with an
 // epilogue applied to each value at its natural index between them.
 
-template <int NA, int DIR, typename T>
-__device__ __forceinline__ void pass_a(T* buf, const LineGeom& g, const T* tw) {
+template <int NA, int DIR, typename T, typename LoadSel = AllPositions, typename StoreSel = AllPositions>
+__device__ __forceinline__ void pass_a(T* buf, const LineGeom& g, const T* tw, const LoadSel& lsel = {},
+                                       const StoreSel& ssel = {}) {
     const int tws = g.n / NA;
     line_pass<NA, false>(buf, g, [&](T* x, int, int q) {
         dft<NA, DIR>(x, tw, tws);
@@ -205,7 +228,7 @@ __device__ __forceinline__ void pass_a(T* buf, const LineGeom& g, const T* tw) {
             for (int k = 1; k < NA; ++k)
                 if (q != 0) x[k] = cmul(x[k], twiddle<DIR>(tw, q * k));  // q*k < n
         }
-    });
+    }, lsel, ssel);
 }
 
 template <int NB, int DIR, typename T>
@@ -240,12 +263,13 @@ __device__ __forceinline__ void pass_mid(T* buf, const LineGeom& g, const T* tw,
 
 // MAXR: the largest factor a caller instantiates (lengths with a larger
 // factor are not transformed); a smaller bound keeps registers down.
-template <int DIR, int MAXR, typename T>
-__device__ __forceinline__ void run_a(T* buf, const LineGeom& g, const T* tw) {
+template <int DIR, int MAXR, typename T, typename LoadSel = AllPositions, typename StoreSel = AllPositions>
+__device__ __forceinline__ void run_a(T* buf, const LineGeom& g, const T* tw, const LoadSel& lsel = {},
+                                      const StoreSel& ssel = {}) {
     switch (g.na) {
 #define Q3B_A(N) \
-    case N:                                                 \
-        if constexpr (N <= MAXR) pass_a<N, DIR>(buf, g, tw); \
+    case N:                                                             \
+        if constexpr (N <= MAXR) pass_a<N, DIR>(buf, g, tw, lsel, ssel); \
         break;
         Q3B_FFT_SIZES(Q3B_A)
 #undef Q3B_A
@@ -288,9 +312,13 @@ __device__ __forceinline__ void forward(T* buf, const LineGeom& g, const T* tw) 
 
 // Backward transform, epi(line, natural index, value) on every value, forward
 // transform; natural order in and out.  Three passes, ends with a barrier.
-template <int MAXR, typename T, typename Epi>
-__device__ __forceinline__ void roundtrip(T* buf, const LineGeom& g, const T* tw, const Epi& epi) {
-    run_a<+1, MAXR>(buf, g, tw);
+// `sel` marks the positions that hold data on input and are wanted on output
+// (the others are read as zero and not written back), for the stride-nb
+// passes (see ItemMask).
+template <int MAXR, typename T, typename Epi, typename Sel = AllPositions>
+__device__ __forceinline__ void roundtrip(T* buf, const LineGeom& g, const T* tw, const Epi& epi,
+                                          const Sel& sel = {}) {
+    run_a<+1, MAXR>(buf, g, tw, sel, AllPositions{});
     __syncthreads();
     switch (g.nb) {
 #define Q3B_M(N) \
@@ -302,7 +330,7 @@ __device__ __forceinline__ void roundtrip(T* buf, const LineGeom& g, const T* tw
         default: break;
     }
     __syncthreads();
-    run_a<-1, MAXR>(buf, g, tw);
+    run_a<-1, MAXR>(buf, g, tw, AllPositions{}, sel);
     __syncthreads();
 }
 

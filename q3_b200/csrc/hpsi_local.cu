@@ -15,6 +15,33 @@ namespace q3b {
 namespace {
 
 constexpr int kStickThreads = 256;
+constexpr int kRowMaskWords = 16;  // one word per item of the first column pass (nb1 <= 16)
+
+// Shared-memory set-up of the plane kernels: rowb[i] = w1 * p2 of the i-th
+// row holding sticks; colmask[q] bit r set when row q + nb1*r holds sticks
+// (the ItemMask of the column passes).  Ends with a barrier.
+template <typename R>
+__device__ __forceinline__ void stick_rows_setup(const LocalPlan<R>& p, int* rowb, unsigned* colmask) {
+    for (int i = threadIdx.x; i < kRowMaskWords; i += blockDim.x) colmask[i] = 0u;
+    __syncthreads();
+    for (int i = threadIdx.x; i < p.nrows; i += blockDim.x) {
+        const int b = p.row_base[i];
+        rowb[i] = b;
+        const int w1 = b / p.p2;
+        atomicOr(&colmask[w1 % p.nb1], 1u << (w1 / p.nb1));
+    }
+    __syncthreads();
+}
+
+// zero the rows that hold sticks, a warp per row
+template <typename T, typename R>
+__device__ __forceinline__ void zero_stick_rows(const LocalPlan<R>& p, const int* rowb, T* plane) {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int r = threadIdx.x >> 5; r < p.nrows; r += nw) {
+        T* row = plane + rowb[r];
+        for (int c = lane; c < p.p2; c += 32) row[c] = czero<T>();
+    }
+}
 
 // V/N of one plane in the layout the plane kernel meets it: [w1][w2 position]
 // with the w2 positions of the digit-reversed order the row transform leaves.
@@ -79,11 +106,14 @@ __global__ void __launch_bounds__(NT, (plane_min_blocks<R, NT, MAXR>())) planes(
     T* tw2 = tw1 + p.n1;
     T* plane = tw2 + p.n2;
     int* rowb = reinterpret_cast<int*>(plane + (long)p.n1 * p.p2);
+    unsigned* colmask = reinterpret_cast<unsigned*>(rowb + p.nrows);  // see stick_rows_setup
     const int i3 = blockIdx.x, band = blockIdx.y;
     for (int i = threadIdx.x; i < p.n1; i += NT) tw1[i] = p.tw1[i];
     for (int i = threadIdx.x; i < p.n2; i += NT) tw2[i] = p.tw2[i];
-    for (int i = threadIdx.x; i < p.nrows; i += NT) rowb[i] = p.row_base[i];
-    for (int i = threadIdx.x; i < p.n1 * p.p2; i += NT) plane[i] = czero<T>();
+    stick_rows_setup(p, rowb, colmask);
+    // only the rows that hold sticks are read before they are written: the
+    // column transform reads the others as zero, and writes back only these
+    zero_stick_rows(p, rowb, plane);
     __syncthreads();
     T* xp = X + ((long)band * p.n3 + i3) * p.nsticks;
     for (int s = threadIdx.x; s < p.nsticks; s += NT) plane[p.stick_pos[s]] = xp[s];
@@ -91,7 +121,8 @@ __global__ void __launch_bounds__(NT, (plane_min_blocks<R, NT, MAXR>())) planes(
     fft::LineGeom gr{p.n2, p.na2, p.nb2, p.nrows, 0, 1, rowb};
     fft::LineGeom gc{p.n1, p.na1, p.nb1, p.n2, 1, p.p2, nullptr};
     fft::backward<MAXR>(plane, gr, tw2);
-    fft::roundtrip<MAXR>(plane, gc, tw1, VEpilogue<R>{p.vplane + (long)i3 * p.n1 * p.n2, p.n2});
+    fft::roundtrip<MAXR>(plane, gc, tw1, VEpilogue<R>{p.vplane + (long)i3 * p.n1 * p.n2, p.n2},
+                         fft::ItemMask{colmask});
     fft::forward<MAXR>(plane, gr, tw2);
     for (int s = threadIdx.x; s < p.nsticks; s += NT) xp[s] = plane[p.stick_pos[s]];
 }
@@ -171,11 +202,77 @@ void launch_planes(dim3 grid, size_t smem, cudaStream_t st, const LocalPlan<R>& 
     planes<R, NT, MAXR><<<grid, NT, smem, st>>>(p, X);
 }
 
+// Charge density (accumulator.hpp:375-545, non-Gamma): the backward half of
+// the plane pass.  Block (plane position i3, band group g) transforms each
+// band of its group on plane i3 (rows holding sticks, then all columns, both
+// left in digit-reversed order) and adds w_b |psi(r)|^2 into its own slab of
+// `partial` ([g][i3][w1 pos][w2 pos]); one block per slab, bands in order, so
+// the sums are deterministic.  Bands of weight 0 are skipped.
+template <int MAXR>
+__global__ void __launch_bounds__(256) planes_density(LocalPlan<double> p, const double2* X, int nb,
+                                                      const double* w, double* partial, int groups) {
+    using T = double2;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* tw1 = reinterpret_cast<T*>(smem);
+    T* tw2 = tw1 + p.n1;
+    T* plane = tw2 + p.n2;
+    int* rowb = reinterpret_cast<int*>(plane + (long)p.n1 * p.p2);
+    unsigned* colmask = reinterpret_cast<unsigned*>(rowb + p.nrows);
+    const int i3 = blockIdx.x, g = blockIdx.y;
+    const int per = (nb + groups - 1) / groups;
+    const int b0 = g * per, b1 = min(nb, b0 + per);
+    for (int i = threadIdx.x; i < p.n1; i += blockDim.x) tw1[i] = p.tw1[i];
+    for (int i = threadIdx.x; i < p.n2; i += blockDim.x) tw2[i] = p.tw2[i];
+    stick_rows_setup(p, rowb, colmask);
+    const int nplane = p.n1 * p.n2;
+    double* acc = partial + ((size_t)g * p.n3 + i3) * nplane;
+    fft::LineGeom gr{p.n2, p.na2, p.nb2, p.nrows, 0, 1, rowb};
+    fft::LineGeom gc{p.n1, p.na1, p.nb1, p.n2, 1, p.p2, nullptr};
+    for (int b = b0; b < b1; ++b) {
+        const double wb = w[b];
+        if (wb == 0.0) continue;
+        zero_stick_rows(p, rowb, plane);
+        __syncthreads();
+        const T* xp = X + ((long)b * p.n3 + i3) * p.nsticks;
+        for (int s = threadIdx.x; s < p.nsticks; s += blockDim.x) plane[p.stick_pos[s]] = xp[s];
+        __syncthreads();
+        fft::backward<MAXR>(plane, gr, tw2);
+        fft::run_a<+1, MAXR>(plane, gc, tw1, fft::ItemMask{colmask}, fft::AllPositions{});
+        __syncthreads();
+        fft::run_b<+1, MAXR>(plane, gc, tw1);
+        __syncthreads();
+        for (int i = threadIdx.x; i < nplane; i += blockDim.x) {
+            const T v = plane[(i / p.n2) * p.p2 + i % p.n2];
+            acc[i] += wb * (v.x * v.x + v.y * v.y);
+        }
+        __syncthreads();
+    }
+}
+
+// rho[(w1*N2 + w2)*N3 + w3] += sum over groups (in order) of the partial at
+// the digit-reversed positions of (w1, w2, w3)
+__global__ void density_reduce(LocalPlan<double> p, int groups, const double* partial, double* rho) {
+    const long n = (long)p.n1 * p.n2 * p.n3;
+    const long nplane = (long)p.n1 * p.n2;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+        const int w3 = static_cast<int>(idx % p.n3);
+        const int w2 = static_cast<int>((idx / p.n3) % p.n2);
+        const int w1 = static_cast<int>(idx / ((long)p.n3 * p.n2));
+        const int q1 = p.nb1 * (w1 % p.na1) + w1 / p.na1;
+        const int q2 = p.nb2 * (w2 % p.na2) + w2 / p.na2;
+        const int q3 = p.nb3 * (w3 % p.na3) + w3 / p.na3;
+        const long off = (long)q3 * nplane + (long)q1 * p.n2 + q2;
+        double s = 0.0;
+        for (int g = 0; g < groups; ++g) s += partial[(long)g * p.n3 * nplane + off];
+        rho[idx] += s;
+    }
+}
+
 }  // namespace
 
 template <typename R> size_t plane_smem_bytes(const LocalPlan<R>& p) {
     return (size_t)(p.n1 + p.n2 + (size_t)p.n1 * p.p2) * sizeof(cplx_t<R>) +
-           (size_t)p.nrows * sizeof(int);
+           (size_t)p.nrows * sizeof(int) + kRowMaskWords * sizeof(unsigned);
 }
 
 PhaseTimer::PhaseTimer() {
@@ -260,6 +357,52 @@ void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, l
         kinetic_unmapped<R><<<blocks, 256, 0, st>>>(p, psi, ldpsi, hpsi, ldh, nvec);
         Q3B_LAUNCH_CHECK();
     }
+}
+
+int density_groups(const LocalPlan<double>& p, int nvec) {
+    int g = (2 * 148 + p.n3 - 1) / p.n3;
+    if (g > nvec) g = nvec;
+    return g < 1 ? 1 : g;
+}
+
+void accumulate_density(cudaStream_t st, const LocalPlan<double>& p, const double2* psi, long ldpsi, int nvec,
+                        const double* w, double2* X, int chunk, double* partial, int groups, double* rho) {
+    if (nvec <= 0 || p.nsticks == 0) return;
+    set_smem_limits<double>();
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaFuncSetAttribute(planes_density<kSmallR>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(planes_density<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    });
+    if (chunk < 1) chunk = 1;
+    const size_t smem_s = stick_smem_bytes(p);
+    const size_t smem_p = plane_smem_bytes(p);
+    const int nsg = ceil_div(p.nsticks, p.sg);
+    const bool small3 = p.na3 <= kSmallR && p.nb3 <= kSmallR;
+    const bool small12 = p.na1 <= kSmallR && p.nb1 <= kSmallR && p.na2 <= kSmallR && p.nb2 <= kSmallR;
+    Q3B_CUDA(cudaMemsetAsync(partial, 0, (size_t)groups * p.n1 * p.n2 * p.n3 * sizeof(double), st));
+    for (int b0 = 0; b0 < nvec; b0 += chunk) {
+        const int nb = nvec - b0 < chunk ? nvec - b0 : chunk;
+        const double2* ps = psi + (long)b0 * ldpsi;
+        if (small3)
+            sticks_backward<double, kSmallR><<<dim3(nsg, nb), kStickThreads, smem_s, st>>>(p, ps, ldpsi, X);
+        else
+            sticks_backward<double, 16><<<dim3(nsg, nb), kStickThreads, smem_s, st>>>(p, ps, ldpsi, X);
+        Q3B_LAUNCH_CHECK();
+        const int gb = nb < groups ? nb : groups;
+        // every chunk adds into the same slabs; a chunk with fewer bands than
+        // groups leaves the remaining slabs as they are
+        if (small12)
+            planes_density<kSmallR><<<dim3(p.n3, gb), 256, smem_p, st>>>(p, X, nb, w + b0, partial, gb);
+        else
+            planes_density<16><<<dim3(p.n3, gb), 256, smem_p, st>>>(p, X, nb, w + b0, partial, gb);
+        Q3B_LAUNCH_CHECK();
+    }
+    const long n = (long)p.n1 * p.n2 * p.n3;
+    int blocks = ceil_div(n, 256);
+    if (blocks > 4096) blocks = 4096;
+    density_reduce<<<blocks, 256, 0, st>>>(p, groups, partial, rho);
+    Q3B_LAUNCH_CHECK();
 }
 
 template void apply_local<double>(cudaStream_t, const LocalPlan<double>&, const double2*, long,

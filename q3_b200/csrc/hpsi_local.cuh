@@ -71,6 +71,15 @@ void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, l
                  cplx_t<R>* hpsi, long ldh, int nvec, cplx_t<R>* X, int chunk,
                  PhaseTimer* timer = nullptr);
 
+// Charge density: rho (N doubles, natural grid order) += sum_b w[b] |psi_b(r)|^2,
+// psi_b(r) the unnormalised backward transform of band b scattered onto the
+// grid.  w: nvec device weights (0 skips a band).  X: chunk *
+// sticks_bytes_per_band; partial: groups * N doubles with groups from
+// density_groups().
+int density_groups(const LocalPlan<double>& p, int nvec);
+void accumulate_density(cudaStream_t st, const LocalPlan<double>& p, const double2* psi, long ldpsi, int nvec,
+                        const double* w, double2* X, int chunk, double* partial, int groups, double* rho);
+
 // shared-memory footprint of the plane kernel (for capacity checks)
 template <typename R> size_t plane_smem_bytes(const LocalPlan<R>& p);
 

@@ -194,3 +194,25 @@ def test_starting_rotation_oracle_matches_reference_kat():
     w, bands = ostart.starting_subspace(lambda x: diag[:, None] * x, chi, nb)
     assert np.all(w >= diag[:nb] - 1e-12)
     assert np.max(np.abs(bands.conj().T @ bands - np.eye(nb))) < 1e-12
+
+
+def test_density_oracle_plane_wave_and_charge():
+    """One plane wave of unit coefficient has |psi(r)| = 1 at every grid point
+    after the unnormalised backward transform, so rho = w everywhere; and the
+    total charge of orthonormal bands is sum_b f_b (the reference's
+    test_accumulator.cpp:43-99 check, at 1e-12 instead of 0.01)."""
+    from oracle import density as odens
+    grid = (6, 5, 4)
+    n = int(np.prod(grid))
+    psi = np.zeros((3, 1), dtype=np.complex128)
+    psi[1, 0] = 1.0
+    g2g = np.array([-1, 37, 5])
+    rho = odens.accumulate(psi, g2g, grid, np.array([0.25]))
+    assert np.allclose(rho, 0.25, atol=1e-14)
+    rng = np.random.default_rng(2)
+    q, _ = np.linalg.qr(rng.standard_normal((40, 4)) + 1j * rng.standard_normal((40, 4)))
+    g2g = rng.permutation(n)[:40]
+    f = np.array([2.0, 2.0, 1.0, 0.0])
+    rho = odens.accumulate(q, g2g, grid, f)
+    assert abs(rho.sum() / n - f.sum()) < 1e-12
+    assert rho.min() >= 0.0
