@@ -260,6 +260,13 @@ int q3b_server_wait(q3b_server* server, int id, q3b_cplx128* bands_out, double* 
 int q3b_hegv(q3b_context* ctx, int n, const q3b_cplx128* h_dev, const q3b_cplx128* s_dev, int ld,
              double* w_dev, q3b_cplx128* evec_dev);
 
+/* Counters of the context's CUDA-graph replays of the dense eigensolver: graphs
+ * captured and replays served (either pointer may be NULL).  The launch
+ * sequence of q3b_hegv and of the Davidson subspace solves of order >= 256 is
+ * captured the third time the same problem shape meets the same buffers and
+ * replayed after that.  No counterpart in the reference (diagnostics). */
+int q3b_graph_stats(q3b_context* ctx, int* captures, int* replays);
+
 /* ---- charge density (PlanewaveChargeDensityAccumulator) --------------------- */
 
 /* accumulate_on_rho_grid, non-Gamma branch

@@ -1,3 +1,4 @@
+#include <type_traits>
 #include <algorithm>
 // extern "C" entry points of libq3b (include/q3b.h).  Every call converts
 // exceptions to a status code and keeps the message on the context.
@@ -34,6 +35,16 @@ void gemm_entry(Context& c, char ta, char tb, int m, int n, int k, CT alpha, con
     if (lda < (conj ? k : m) || ldb < k || ldc < m || lda < 1 || ldb < 1)
         throw q3b::Status(Q3B_ERR_INVALID, "gemm: leading dimension too small");
     q3b::GemmWorkspace ws = c.gemm_ws(conj ? q3b::cgemm_workspace_bytes<R>(m, n, k) : 0);
+    if constexpr (std::is_same<R, float>::value) {
+        // the single-precision entry point always runs on the tensor cores
+        // (the library's own products route small ones to the CUDA cores)
+        if (k > 0) {
+            q3b::tc::cgemm(c.stream, conj, m, n, k, T{alpha.re, alpha.im}, reinterpret_cast<const T*>(a), lda,
+                           reinterpret_cast<const T*>(b), ldb, T{beta.re, beta.im}, reinterpret_cast<T*>(cc), ldc,
+                           ws);
+            return;
+        }
+    }
     q3b::cgemm<R>(c.stream, conj, m, n, k, T{alpha.re, alpha.im}, reinterpret_cast<const T*>(a), lda,
                   reinterpret_cast<const T*>(b), ldb, T{beta.re, beta.im}, reinterpret_cast<T*>(cc), ldc, ws);
 }
@@ -184,6 +195,13 @@ int q3b_apply_h_host(q3b_context* ctx, const q3b_cplx128* psi, q3b_cplx128* hpsi
     });
 }
 
+int q3b_graph_stats(q3b_context* ctx, int* captures, int* replays) {
+    if (!ctx) return Q3B_ERR_INVALID;
+    if (captures) *captures = ctx->impl.hegv_graphs.captures;
+    if (replays) *replays = ctx->impl.hegv_graphs.replays;
+    return Q3B_OK;
+}
+
 int q3b_accumulate_density(q3b_context* ctx, const q3b_cplx128* psi, int nvec, const double* weights,
                            double* rho) {
     return guarded(ctx, [&](Context& c) {
@@ -299,7 +317,7 @@ int q3b_hegv(q3b_context* ctx, int n, const q3b_cplx128* h, const q3b_cplx128* s
         q3b::GemmWorkspace g = c.gemm_ws(q3b::cgemm_workspace_bytes<double>(n, n, n));
         const int info = q3b::dense::hegv(c.stream, n, reinterpret_cast<const double2*>(h),
                                           reinterpret_cast<const double2*>(s), ld, w,
-                                          reinterpret_cast<double2*>(evec), n, ws, g);
+                                          reinterpret_cast<double2*>(evec), n, ws, g, &c.hegv_graphs);
         Q3B_CUDA(cudaStreamSynchronize(c.stream));
         if (info != 0)
             throw q3b::Status(Q3B_ERR_LINALG, "overlap matrix not positive definite (info " +

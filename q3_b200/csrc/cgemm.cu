@@ -1,3 +1,4 @@
+#include <algorithm>
 // Complex GEMMs on CUDA cores; see cgemm.cuh.
 #include <type_traits>
 
@@ -171,10 +172,13 @@ template <typename R> int choose_splits(int M, int N, int K) {
 
 }  // namespace
 
+bool use_tensor_cores(int M, int N, int K) { return (double)M * N * K >= kTensorCoreMinMacs; }
+
 template <typename R> size_t cgemm_workspace_bytes(int M, int N, int K) {
-    if constexpr (std::is_same<R, float>::value) return tc::workspace_bytes(M, N, K);
     const int s = choose_splits<R>(M, N, K);
-    return s > 1 ? (size_t)s * M * N * sizeof(cplx_t<R>) : 0;
+    const size_t simt = s > 1 ? (size_t)s * M * N * sizeof(cplx_t<R>) : 0;
+    if constexpr (std::is_same<R, float>::value) return std::max(simt, tc::workspace_bytes(M, N, K));
+    return simt;
 }
 
 template <typename R>
@@ -185,7 +189,10 @@ void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, cplx_t<R> alpha, c
     if (M <= 0 || N <= 0) return;
     constexpr int BK = GemmTile<R>::BK;
     if constexpr (std::is_same<R, float>::value) {
-        if (K > 0) {
+        // small products stay on the CUDA cores: a tensor-core block takes a
+        // whole SM's shared memory, which small problems, often several at
+        // once on separate streams, cannot keep busy
+        if (K > 0 && use_tensor_cores(M, N, K)) {
             tc::cgemm(st, conj_a, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, ws);
             return;
         }

@@ -28,6 +28,11 @@ void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, cplx_t<R> alpha, c
 // bytes of workspace cgemm may use for a C,N product of this shape
 template <typename R> size_t cgemm_workspace_bytes(int M, int N, int K);
 
+// FP32 products of at least this many complex multiply-adds (M N K) run on
+// the tensor cores, smaller ones on the CUDA cores
+constexpr double kTensorCoreMinMacs = 67108864.0;  // 2^26
+bool use_tensor_cores(int M, int N, int K);
+
 // The FP32 products run on the tensor cores (cgemm_tc.cu).
 namespace tc {
 void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, const float2* A, long lda,

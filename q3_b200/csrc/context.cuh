@@ -8,6 +8,7 @@
 
 #include "cgemm.cuh"
 #include "common.cuh"
+#include "dense.cuh"
 #include "hpsi_local.cuh"
 #include "nonlocal.cuh"
 
@@ -75,6 +76,8 @@ class Context {
     // workspaces
     DevBuf ws_sticks, ws_gemm, ws_bm, ws_bp, ws_conv_in, ws_conv_out, ws_host_io;
     DevBuf ws_solver, ws_dense, ws_bands, ws_tune;
+    // replays of the dense eigensolver's launch sequence (one per context)
+    dense::HegvGraphs hegv_graphs;
     // charge density: per-group partial sums and the band weights
     DevBuf ws_density;
     // starting-subspace rotation: chi and H chi of the last q3b_start_apply

@@ -315,7 +315,7 @@ template <typename R> class Davidson {
         dscratch_.used = 0;
         const int nvec = std::min(nb_, n);
         GemmWorkspace gws = c_.gemm_ws(cgemm_workspace_bytes<double>(n, n, n));
-        const int info = dense::hegv(st_, n, H, S, ld, w_, evec_, nvec, dscratch_, gws);
+        const int info = dense::hegv(st_, n, H, S, ld, w_, evec_, nvec, dscratch_, gws, &c_.hegv_graphs);
         if (info == 0 && publish) {
             whost_.assign(n, 0.0);
             Q3B_CUDA(cudaMemcpyAsync(whost_.data(), w_, n * sizeof(double), cudaMemcpyDeviceToHost, st_));

@@ -854,7 +854,7 @@ Chol chol_take(Scratch& ws, int n) {
     return c;
 }
 
-int potrf_impl(cudaStream_t st, int n, double2* A, int lda, const Chol& c) {
+void potrf_launch(cudaStream_t st, int n, double2* A, int lda, const Chol& c) {
     const int nblk = ceil_div(n, NB);
     Q3B_CUDA(cudaMemsetAsync(c.info, 0, sizeof(int), st));
     for (int k = 0; k < nblk; ++k) {
@@ -868,6 +868,10 @@ int potrf_impl(cudaStream_t st, int n, double2* A, int lda, const Chol& c) {
             Q3B_LAUNCH_CHECK();
         }
     }
+}
+
+int potrf_impl(cudaStream_t st, int n, double2* A, int lda, const Chol& c) {
+    potrf_launch(st, n, A, lda, c);
     int info = 0;
     Q3B_CUDA(cudaMemcpyAsync(&info, c.info, sizeof(int), cudaMemcpyDeviceToHost, st));
     Q3B_CUDA(cudaStreamSynchronize(st));
@@ -916,105 +920,250 @@ void trtri_after_potrf(cudaStream_t st, int n, const double2* A, int lda, double
     trtri_impl(st, n, A, lda, c, Uinv);
 }
 
-void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, Scratch& ws,
-          const GemmWorkspace& gws) {
-    if (n <= 0) return;
+namespace {
+
+// Everything heev's launches need, taken from the scratch in a fixed order:
+// planning twice from the same scratch state gives the same pointers, which
+// the graph replays of hegv rely on.
+struct HeevPlan {
+    int n = 0, nvec = 0;
+    double* d;
+    double2* e;
+    double2* W;
+    double2* xpre;
+    double2* pbuf;
+    double* ea;
+    double* e2;
+    double2* phase;
+    double* bounds;
+    double* Y;
+    double* work;
+    double2* Yc;
+    double2* partial;
+    unsigned* bar;
+    int* err;
+    int G = 1, cpb = 1, w_in_smem = 0;
+    size_t smem = 0;
+};
+
+HeevPlan heev_plan(int n, int nvec, Scratch& ws) {
+    HeevPlan p;
+    p.n = n;
+    p.nvec = nvec;
     const int nv = nvec > 0 ? nvec : 1;
-    double* d = ws.take<double>(n);
-    double2* e = ws.take<double2>(n);
-    double2* W = ws.take<double2>((size_t)n * n);
-    double2* xpre = ws.take<double2>(2 * (size_t)n);
-    double2* pbuf = ws.take<double2>(2 * (size_t)n);
-    double* ea = ws.take<double>(n);
-    double* e2 = ws.take<double>(n);
-    double2* phase = ws.take<double2>(n);
-    double* bounds = ws.take<double>(4);
-    double* Y = ws.take<double>((size_t)n * nv);
-    double* work = ws.take<double>((size_t)5 * n * nv);
-    double2* Yc = ws.take<double2>((size_t)n * nv);
+    p.d = ws.take<double>(n);
+    p.e = ws.take<double2>(n);
+    p.W = ws.take<double2>((size_t)n * n);
+    p.xpre = ws.take<double2>(2 * (size_t)n);
+    p.pbuf = ws.take<double2>(2 * (size_t)n);
+    p.ea = ws.take<double>(n);
+    p.e2 = ws.take<double>(n);
+    p.phase = ws.take<double2>(n);
+    p.bounds = ws.take<double>(4);
+    p.Y = ws.take<double>((size_t)n * nv);
+    p.work = ws.take<double>((size_t)5 * n * nv);
+    p.Yc = ws.take<double2>((size_t)n * nv);
     int device = 0;
     Q3B_CUDA(cudaGetDevice(&device));
     int nsm = 0;
     Q3B_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     // blocks: about 8 columns each, at most one per SM; columns (and W) in shared memory
-    int G = std::max(1, std::min(nsm, (n + 7) / 8));
-    int cpb = (n + G - 1) / G;
+    p.G = std::max(1, std::min(nsm, (n + 7) / 8));
+    p.cpb = (n + p.G - 1) / p.G;
     const size_t limit = 200 * 1024;
-    size_t smem = ((size_t)cpb * n + 3 * (size_t)n) * sizeof(double2);
-    if (smem > limit) throw Status(Q3B_ERR_INVALID, "subspace of order " + std::to_string(n) + " too large for the eigensolver");
-    int w_in_smem = (smem + (size_t)cpb * n * sizeof(double2) <= limit) ? 1 : 0;
-    if (w_in_smem) smem += (size_t)cpb * n * sizeof(double2);
-    double2* partial = ws.take<double2>(2 * (size_t)G);
-    unsigned* bar = ws.take<unsigned>(2);
-    int* err = ws.take<int>(1);
-    Q3B_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
-    Q3B_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    p.smem = ((size_t)p.cpb * n + 3 * (size_t)n) * sizeof(double2);
+    if (p.smem > limit)
+        throw Status(Q3B_ERR_INVALID, "subspace of order " + std::to_string(n) + " too large for the eigensolver");
+    p.w_in_smem = (p.smem + (size_t)p.cpb * n * sizeof(double2) <= limit) ? 1 : 0;
+    if (p.w_in_smem) p.smem += (size_t)p.cpb * n * sizeof(double2);
+    p.partial = ws.take<double2>(2 * (size_t)p.G);
+    p.bar = ws.take<unsigned>(2);
+    p.err = ws.take<int>(1);
     static std::once_flag once;
     std::call_once(once, [limit] {
         cudaFuncSetAttribute(hetrd_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit);
+        cudaFuncSetAttribute(tridiag_invit_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvitSmemLimit);
     });
     int per_sm = 0;
-    Q3B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_smem, 256, smem));
-    if (per_sm < 1 || per_sm * nsm < G) throw Status(Q3B_ERR_INVALID, "eigensolver blocks cannot be co-resident");
-    const double2* Ac = A;
-    void* args[] = {&n, &cpb, &w_in_smem, &Ac, &d, &e, &W, &xpre, &pbuf, &partial, &bar, &err};
-    Q3B_CUDA(cudaLaunchCooperativeKernel((const void*)hetrd_smem, dim3(G), dim3(256), args, smem, st));
+    Q3B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_smem, 256, p.smem));
+    if (per_sm < 1 || per_sm * nsm < p.G) throw Status(Q3B_ERR_INVALID, "eigensolver blocks cannot be co-resident");
+    return p;
+}
+
+// heev's launches, no host synchronisation (the timeout word is read by the caller)
+void heev_launch(cudaStream_t st, const HeevPlan& p, const double2* A, double* w, double2* Z,
+                 const GemmWorkspace& gws) {
+    const int n = p.n, nvec = p.nvec;
+    Q3B_CUDA(cudaMemsetAsync(p.bar, 0, 2 * sizeof(unsigned), st));
+    Q3B_CUDA(cudaMemsetAsync(p.err, 0, sizeof(int), st));
+    {
+        int nn = n, cpb = p.cpb, wis = p.w_in_smem;
+        const double2* Ac = A;
+        double* d = p.d;
+        double2 *e = p.e, *W = p.W, *xpre = p.xpre, *pbuf = p.pbuf, *partial = p.partial;
+        unsigned* bar = p.bar;
+        int* err = p.err;
+        void* args[] = {&nn, &cpb, &wis, &Ac, &d, &e, &W, &xpre, &pbuf, &partial, &bar, &err};
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(p.G);
+        cfg.blockDim = dim3(256);
+        cfg.dynamicSmemBytes = p.smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        Q3B_CUDA(cudaLaunchKernelExC(&cfg, (const void*)hetrd_smem, args));
+        Q3B_LAUNCH_CHECK();
+    }
+    tridiag_prep<<<1, 32, 0, st>>>(n, p.d, p.e, p.ea, p.e2, p.phase, p.bounds);
     Q3B_LAUNCH_CHECK();
-    tridiag_prep<<<1, 32, 0, st>>>(n, d, e, ea, e2, phase, bounds);
-    Q3B_LAUNCH_CHECK();
-    tridiag_multisect<<<ceil_div((long)n * 32, 256), 256, 0, st>>>(n, d, e2, bounds, w);
+    tridiag_multisect<<<ceil_div((long)n * 32, 256), 256, 0, st>>>(n, p.d, p.e2, p.bounds, w);
     Q3B_LAUNCH_CHECK();
     if (nvec > 0) {
         const int T = static_cast<int>(std::min<size_t>(64, kInvitSmemLimit / ((size_t)n * kInvitBytesPerRow)));
         if (T >= 1) {
-            static std::once_flag once_inv;
-            std::call_once(once_inv, [] {
-                cudaFuncSetAttribute(tridiag_invit_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kInvitSmemLimit);
-            });
             const size_t sm = (size_t)n * T * kInvitBytesPerRow;
-            tridiag_invit_smem<<<ceil_div(nvec, T), T, sm, st>>>(n, d, ea, w, bounds, nvec, Y);
+            tridiag_invit_smem<<<ceil_div(nvec, T), T, sm, st>>>(n, p.d, p.ea, w, p.bounds, nvec, p.Y);
         } else {
-            tridiag_invit<<<ceil_div(nvec, 64), 64, 0, st>>>(n, d, ea, w, bounds, nvec, Y, work);
+            tridiag_invit<<<ceil_div(nvec, 64), 64, 0, st>>>(n, p.d, p.ea, w, p.bounds, nvec, p.Y, p.work);
         }
         Q3B_LAUNCH_CHECK();
-        apply_phase<<<grid_for((long)n * nvec), 256, 0, st>>>(n, nvec, phase, Y, Yc);
+        apply_phase<<<grid_for((long)n * nvec), 256, 0, st>>>(n, nvec, p.phase, p.Y, p.Yc);
         Q3B_LAUNCH_CHECK();
         const double2 one = mk(1.0, 0.0), zero = mk(0.0, 0.0);
-        cgemm<double>(st, true, n, nvec, n, one, W, n, Yc, n, zero, Z, n, gws);   // Z = W^H (D Y)
+        cgemm<double>(st, true, n, nvec, n, one, p.W, n, p.Yc, n, zero, Z, n, gws);   // Z = W^H (D Y)
     }
-    int herr = 0;
-    Q3B_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+}
+
+int read_flag(cudaStream_t st, const int* flag) {
+    int h = 0;
+    Q3B_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
     Q3B_CUDA(cudaStreamSynchronize(st));
-    if (herr) throw Status(Q3B_ERR_INTERNAL, "eigensolver grid barrier timed out");
+    return h;
+}
+
+}  // namespace
+
+void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, Scratch& ws,
+          const GemmWorkspace& gws) {
+    if (n <= 0) return;
+    const HeevPlan p = heev_plan(n, nvec, ws);
+    heev_launch(st, p, A, w, Z, gws);
+    if (read_flag(st, p.err)) throw Status(Q3B_ERR_INTERNAL, "eigensolver grid barrier timed out");
+}
+
+HegvGraphs::~HegvGraphs() {
+    for (int i = 0; i < count_; ++i)
+        if (entries_[i].exec) cudaGraphExecDestroy(entries_[i].exec);
+}
+
+bool HegvGraphs::Key::operator==(const Key& o) const {
+    return n == o.n && ld == o.ld && nvec == o.nvec && H == o.H && S == o.S && w == o.w && Z == o.Z &&
+           ws == o.ws && gws == o.gws && ws_used == o.ws_used && ws_bytes == o.ws_bytes &&
+           gws_bytes == o.gws_bytes && st == o.st;
+}
+
+HegvGraphs::Entry* HegvGraphs::find(const Key& k) {
+    for (int i = 0; i < count_; ++i) {
+        if (entries_[i].key == k) {
+            entries_[i].used = ++tick_;
+            if (entries_[i].exec)
+                for (unsigned long long l = 0; l < entries_[i].launches; ++l) count_launch();
+            return &entries_[i];
+        }
+    }
+    return nullptr;
+}
+
+void HegvGraphs::store(const Key& k, cudaGraphExec_t e) {
+    int slot = count_;
+    if (count_ == kMax) {
+        slot = 0;
+        for (int i = 1; i < kMax; ++i)
+            if (entries_[i].used < entries_[slot].used) slot = i;
+        if (entries_[slot].exec) cudaGraphExecDestroy(entries_[slot].exec);
+    } else {
+        ++count_;
+    }
+    entries_[slot] = Entry{k, e, ++tick_, 0, 1};
+}
+
+cudaGraphExec_t HegvGraphs::capture(cudaStream_t st, void (*issue)(void*), void* ctx) {
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        disabled = true;
+        return nullptr;
+    }
+    const unsigned long long l0 = launches();
+    bool ok = true;
+    try {
+        issue(ctx);
+    } catch (const std::exception&) {
+        ok = false;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    cudaGraphExec_t exec = nullptr;
+    if (ok && e == cudaSuccess && g && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess) {
+        captured_launches_ = launches() - l0;
+    } else {
+        exec = nullptr;
+        disabled = true;
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return exec;
 }
 
 int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, double* w, double2* Z,
-         int nvec, Scratch& ws, const GemmWorkspace& gws) {
+         int nvec, Scratch& ws, const GemmWorkspace& gws, HegvGraphs* graphs) {
     if (n <= 0) return 0;
+    const size_t used0 = ws.used;
     const size_t nn = (size_t)n * n;
+    // every slice first, in a fixed order: the same pointers on every call
     double2* Uw = ws.take<double2>(nn);
     Chol c = chol_take(ws, n);
-    copy_matrix<<<grid_for((long)nn), 256, 0, st>>>(n, S, ld, Uw, n);
-    Q3B_LAUNCH_CHECK();
-    const int info = potrf_impl(st, n, Uw, n, c);
-    if (info != 0) return n + info;
     double2* Ui = ws.take<double2>(nn);
-    trtri_impl(st, n, Uw, n, c, Ui);
     double2* Hf = ws.take<double2>(nn);
-    hermitian_from_upper<<<grid_for((long)nn), 256, 0, st>>>(n, H, ld, Hf);
-    Q3B_LAUNCH_CHECK();
     double2* W = ws.take<double2>(nn);
-    const double2 one = mk(1.0, 0.0), zero = mk(0.0, 0.0);
-    cgemm<double>(st, false, n, n, n, one, Hf, n, Ui, n, zero, W, n, gws);     // H U^{-1}
-    cgemm<double>(st, true, n, n, n, one, Ui, n, W, n, zero, Hf, n, gws);      // U^{-H} H U^{-1}
-    // make it exactly Hermitian from its upper triangle
-    hermitian_from_upper<<<grid_for((long)nn), 256, 0, st>>>(n, Hf, n, W);
-    Q3B_LAUNCH_CHECK();
     double2* Zc = ws.take<double2>((size_t)n * (nvec > 0 ? nvec : 1));
-    heev(st, n, W, w, Zc, nvec, ws, gws);
-    if (nvec > 0) cgemm<double>(st, false, n, nvec, n, one, Ui, n, Zc, n, zero, Z, n, gws);
-    return 0;
+    const HeevPlan hp = heev_plan(n, nvec, ws);
+    auto issue = [&] {
+        const double2 one = mk(1.0, 0.0), zero = mk(0.0, 0.0);
+        copy_matrix<<<grid_for((long)nn), 256, 0, st>>>(n, S, ld, Uw, n);
+        Q3B_LAUNCH_CHECK();
+        potrf_launch(st, n, Uw, n, c);
+        trtri_impl(st, n, Uw, n, c, Ui);
+        hermitian_from_upper<<<grid_for((long)nn), 256, 0, st>>>(n, H, ld, Hf);
+        Q3B_LAUNCH_CHECK();
+        cgemm<double>(st, false, n, n, n, one, Hf, n, Ui, n, zero, W, n, gws);     // H U^{-1}
+        cgemm<double>(st, true, n, n, n, one, Ui, n, W, n, zero, Hf, n, gws);      // U^{-H} H U^{-1}
+        // make it exactly Hermitian from its upper triangle
+        hermitian_from_upper<<<grid_for((long)nn), 256, 0, st>>>(n, Hf, n, W);
+        Q3B_LAUNCH_CHECK();
+        heev_launch(st, hp, W, w, Zc, gws);
+        if (nvec > 0) cgemm<double>(st, false, n, nvec, n, one, Ui, n, Zc, n, zero, Z, n, gws);
+    };
+    cudaGraphExec_t ex = nullptr;
+    if (graphs) {
+        const HegvGraphs::Key key{n, ld, nvec, H, S, w, Z, ws.base, gws.ptr, used0, ws.bytes, gws.bytes, st};
+        ex = graphs->get(key, issue);
+    }
+    if (ex) {
+        Q3B_CUDA(cudaGraphLaunch(ex, st));
+    } else {
+        issue();
+    }
+    // a failed Cholesky leaves the later steps on garbage: their result is
+    // discarded, and every loop in them is bounded
+    int flags[2] = {0, 0};
+    Q3B_CUDA(cudaMemcpyAsync(&flags[0], c.info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    Q3B_CUDA(cudaMemcpyAsync(&flags[1], hp.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    Q3B_CUDA(cudaStreamSynchronize(st));
+    if (flags[1]) throw Status(Q3B_ERR_INTERNAL, "eigensolver grid barrier timed out");
+    return flags[0] ? n + flags[0] : 0;
 }
 
 }  // namespace dense

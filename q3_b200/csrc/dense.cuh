@@ -4,6 +4,8 @@
 // (subspace_manager/serial.hpp:334-339, subspace/serial.hpp:18-151).
 #pragma once
 
+#include <type_traits>
+
 #include "cgemm.cuh"
 #include "common.cuh"
 
@@ -40,12 +42,87 @@ int potrf(cudaStream_t st, int n, double2* A, int lda, Scratch& ws);
 // base and `used`), so that the block inverses potrf stored are found again.
 void trtri_after_potrf(cudaStream_t st, int n, const double2* A, int lda, double2* Uinv, Scratch& ws);
 
+// Captured CUDA graphs of hegv's launch sequence (about 3 n/32 + 15 launches,
+// no host synchronisation inside), keyed by every argument the sequence
+// depends on, the last few kept.  A caller that solves problems of the same
+// shape on the same buffers again and again (a Davidson loop) replays one
+// graph per solve.  If the runtime refuses a capture, graphs are turned off
+// and the launches are issued directly.
+class HegvGraphs {
+  public:
+    HegvGraphs() = default;
+    HegvGraphs(const HegvGraphs&) = delete;
+    HegvGraphs& operator=(const HegvGraphs&) = delete;
+    ~HegvGraphs();
+    struct Key {
+        int n, ld, nvec;
+        const void *H, *S, *w, *Z, *ws, *gws;
+        size_t ws_used, ws_bytes, gws_bytes;
+        cudaStream_t st;
+        bool operator==(const Key& o) const;
+    };
+    // the executable graph for `k`, capturing `issue` on the stream when new;
+    // nullptr when graphs are off
+    template <typename F> cudaGraphExec_t get(const Key& k, F&& issue);
+    bool disabled = false;
+    int captures = 0, replays = 0;
+
+  private:
+    struct Entry {
+        Key key;
+        cudaGraphExec_t exec;
+        unsigned long long used;
+        unsigned long long launches;  // kernels in the graph (the library's launch count)
+        int seen;
+    };
+    static constexpr int kMax = 16;
+    static constexpr int kCaptureAfter = 3;
+    // below this order the sequence is short and the solves are often many
+    // at once on other streams (serving), where instantiating graphs costs
+    // more than the launches it saves
+    static constexpr int kMinOrder = 256;
+    Entry entries_[kMax];
+    int count_ = 0;
+    unsigned long long tick_ = 0;
+    unsigned long long captured_launches_ = 0;
+    cudaGraphExec_t capture(cudaStream_t st, void (*issue)(void*), void* ctx);
+    Entry* find(const Key& k);
+    void store(const Key& k, cudaGraphExec_t e);
+};
+
+// A key is only counted the first kCaptureAfter - 1 times it is seen (the
+// caller launches directly); then it is captured and replayed from there on,
+// so shapes that come and go (a Davidson basis that shrinks as bands
+// converge) pay no capture and instantiation.
+template <typename F> cudaGraphExec_t HegvGraphs::get(const Key& k, F&& issue) {
+    if (disabled || k.n < kMinOrder) return nullptr;
+    Entry* hit = find(k);
+    if (hit && hit->exec) {
+        ++replays;
+        return hit->exec;
+    }
+    if (!hit) {
+        store(k, nullptr);
+        return nullptr;
+    }
+    if (++hit->seen < kCaptureAfter) return nullptr;
+    using FF = std::remove_reference_t<F>;
+    cudaGraphExec_t e = capture(k.st, [](void* f) { (*static_cast<FF*>(f))(); }, &issue);
+    if (e) {
+        hit->exec = e;
+        hit->launches = captured_launches_;
+        ++captures;
+    }
+    return e;
+}
+
 // Generalized Hermitian eigenproblem H c = w S c (itype 1; upper triangles of
 // H and S, ld ld).  Eigenvalues ascending in w (n, device), the first nvec
 // S-orthonormal eigenvectors in Z (n x nvec, ld n).  Returns 0, or n + j
-// when S is not positive definite (zhegv's convention).
+// when S is not positive definite (zhegv's convention).  With `graphs`, the
+// launch sequence is replayed from a captured graph when one matches.
 int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, double* w, double2* Z,
-         int nvec, Scratch& ws, const GemmWorkspace& gws);
+         int nvec, Scratch& ws, const GemmWorkspace& gws, HegvGraphs* graphs = nullptr);
 
 // Standard Hermitian eigenproblem of a full (both triangles) matrix A (n x n,
 // ld n; read only).  Eigenvalues ascending in w, the first nvec eigenvectors

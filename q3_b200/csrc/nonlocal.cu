@@ -61,7 +61,7 @@ void apply_nonlocal(cudaStream_t st, const NonlocalData<R>& nl, int npw, int nve
     const T one = mk(R(1), R(0)), zero = mk(R(0), R(0));
     if (tm) tm->begin(PhaseTimer::PROJ_OVERLAP);
     if constexpr (std::is_same<R, float>::value) {
-        if (nl.beta_overlap.tiles)
+        if (nl.beta_overlap.tiles && use_tensor_cores(nl.nproj, nvec, npw))
             tc::cgemm_packed(st, true, nl.nproj, nvec, npw, one, nl.beta_overlap, psi, ldpsi, zero, Bm, nl.nproj, ws);
         else
             cgemm<R>(st, true, nl.nproj, nvec, npw, one, nl.beta, npw, psi, ldpsi, zero, Bm, nl.nproj, ws);
@@ -76,7 +76,7 @@ void apply_nonlocal(cudaStream_t st, const NonlocalData<R>& nl, int npw, int nve
     if (tm) tm->end();
     if (tm) tm->begin(PhaseTimer::PROJ_ACCUM);
     if constexpr (std::is_same<R, float>::value) {
-        if (nl.beta_accum.tiles)
+        if (nl.beta_accum.tiles && use_tensor_cores(npw, nvec, nl.nproj))
             tc::cgemm_packed(st, false, npw, nvec, nl.nproj, one, nl.beta_accum, Bp, nl.nproj, one, hpsi, ldh, ws);
         else
             cgemm<R>(st, false, npw, nvec, nl.nproj, one, nl.beta, npw, Bp, nl.nproj, one, hpsi, ldh, ws);

@@ -117,7 +117,7 @@ int q3b_starting_subspace(q3b_context* ctx, const q3b_cplx128* chi_host, int nch
         c.ws_dense.reserve(&c, q3b::dense::hegv_scratch_bytes(n));
         q3b::dense::Scratch ws{c.ws_dense.as<char>(), c.ws_dense.bytes, 0};
         q3b::GemmWorkspace g = c.gemm_ws(q3b::cgemm_workspace_bytes<double>(n, n, n));
-        const int info = q3b::dense::hegv(c.stream, n, H, S, n, w, Z, nb, ws, g);
+        const int info = q3b::dense::hegv(c.stream, n, H, S, n, w, Z, nb, ws, g, &c.hegv_graphs);
         if (info != 0)
             throw q3b::Status(Q3B_ERR_LINALG, "overlap of the starting vectors is not positive definite (info " +
                                                   std::to_string(info) + ")");

@@ -174,3 +174,36 @@ def test_davidson_device_bands(cuda_device, ctx_app):
     res = dv.solve(x, 4)
     host = _gpu_solve(ctx_app, sy, 0, 1e-10, 80)
     assert np.max(np.abs(res.eigenvalues - host.eigenvalues)) < 1e-12
+
+
+@pytest.mark.parametrize("n", [256, 300])
+def test_hegv_graph_replay_is_bitwise_the_direct_solve(cuda_device, ctx_app, n):
+    """Same device buffers five times: the first two solves launch directly,
+    the third captures a CUDA graph, the later ones replay it; every result is
+    bitwise the first."""
+    import ctypes as C
+    import torch
+    rng = np.random.default_rng(n + 5)
+    x = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    h = (x + x.conj().T) / 2
+    q, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    s = np.eye(n) + 1e-3 * (q + q.conj().T) / 2
+    dev = torch.device("cuda", 0)
+    H = torch.from_numpy(np.ascontiguousarray(h.T)).to(dev)
+    S = torch.from_numpy(np.ascontiguousarray(s.T)).to(dev)
+    w = torch.empty(n, dtype=torch.float64, device=dev)
+    Z = torch.empty(n, n, dtype=torch.complex128, device=dev)
+    lib, hdl = ctx_app.lib, ctx_app.h
+    c0, r0 = C.c_int(), C.c_int()
+    lib.q3b_graph_stats(hdl, C.byref(c0), C.byref(r0))
+    out = []
+    for _ in range(5):
+        assert lib.q3b_hegv(hdl, n, H.data_ptr(), S.data_ptr(), n, w.data_ptr(), Z.data_ptr()) == 0
+        out.append((w.cpu().numpy().copy(), Z.cpu().numpy().copy()))
+    c1, r1 = C.c_int(), C.c_int()
+    lib.q3b_graph_stats(hdl, C.byref(c1), C.byref(r1))
+    assert c1.value - c0.value == 1 and r1.value - r0.value == 2
+    for wk, zk in out[1:]:
+        assert np.array_equal(wk, out[0][0]) and np.array_equal(zk, out[0][1])
+    we = odav.diagonalize_subspace(h, s, n)[0]
+    assert np.max(np.abs(out[4][0] - we)) < 1e-12 * max(1.0, np.max(np.abs(we))) * max(1, n / 16)

@@ -216,3 +216,45 @@ def test_density_oracle_plane_wave_and_charge():
     rho = odens.accumulate(q, g2g, grid, f)
     assert abs(rho.sum() / n - f.sum()) < 1e-12
     assert rho.min() >= 0.0
+
+
+def test_projector_oracle_pieces_match_reference_kats():
+    """The pieces of the projector builder against the reference's own tests:
+    test_lagrange.cpp:10-66 (4-point Lagrange on uniform tables),
+    test_harmonics.cpp:16-205, 337-362 (Y_lm closed values, order sequence,
+    (l, m) index, the G = 0 convention), plus orthonormality over the sphere."""
+    from oracle import projectors as op
+    lin = np.array([1.0, 3.0, 5.0, 7.0, 9.0, 11.0])
+    for q, v in ((0.0, 1.0), (1.0, 3.0), (2.0, 5.0), (0.5, 2.0), (1.5, 4.0), (2.3, 5.6)):
+        assert abs(op.lagrange_4point(lin, q, 1.0) - v) < 1e-12
+    sq = np.array([0.0, 1.0, 4.0, 9.0, 16.0, 25.0])
+    for q, v in ((0.5, 0.25), (1.5, 2.25), (2.5, 6.25)):
+        assert abs(op.lagrange_4point(sq, q, 1.0) - v) < 1e-12
+    cu = np.array([0.0, 1.0, 8.0, 27.0, 64.0, 125.0])
+    for q, v in ((0.5, 0.125), (1.5, 3.375), (2.7, 19.683)):
+        assert abs(op.lagrange_4point(cu, q, 1.0) - v) < 1e-10
+    assert op.lagrange_4point(np.array([1.0, 2.0, 3.0]), 1.0, 1.0) == 0.0   # too short
+    assert op.order_sequence(0) == [0] and op.order_sequence(2) == [0, 1, -1, 2, -2]
+    assert [op.lm_index(l, m) for l in range(3) for m in op.order_sequence(l)] == list(range(9))
+    y00 = 1.0 / np.sqrt(4 * np.pi)
+    c1 = np.sqrt(3.0 / (4 * np.pi))
+    ex, ey, ez = np.eye(3)
+    assert abs(op.real_ylm(1, ez)[op.lm_index(1, 0)] - c1) < 1e-14
+    assert abs(op.real_ylm(1, -ez)[op.lm_index(1, 0)] + c1) < 1e-14
+    assert abs(op.real_ylm(1, ex)[op.lm_index(1, 1)] + c1) < 1e-14      # Condon-Shortley: -x/r
+    assert abs(op.real_ylm(1, ey)[op.lm_index(1, -1)] + c1) < 1e-14
+    z = op.real_ylm(2, np.zeros(3))
+    assert abs(z[0] - y00) < 1e-14 and abs(z[op.lm_index(1, 0)]) < 1e-14
+    assert abs(z[op.lm_index(1, 1)]) < 1e-14 and z[op.lm_index(1, -1)] < -1e-3
+    # orthonormal over the sphere (Gauss-Legendre in cos(theta) x uniform phi)
+    lmax = 3
+    x, wx = np.polynomial.legendre.leggauss(24)
+    phis = np.linspace(0, 2 * np.pi, 48, endpoint=False)
+    gram = np.zeros(((lmax + 1) ** 2,) * 2)
+    for ct, w in zip(x, wx):
+        st = np.sqrt(1 - ct * ct)
+        for ph in phis:
+            y = op.real_ylm(lmax, np.array([st * np.cos(ph), st * np.sin(ph), ct]))
+            gram += w * (2 * np.pi / len(phis)) * np.outer(y, y)
+    assert np.max(np.abs(gram - np.eye(len(gram)))) < 1e-12
+    assert op.angular_phase(1) == -1j and op.angular_phase(6) == -1.0
