@@ -93,7 +93,11 @@ int q3b_prepare_kpoint(q3b_context* ctx, int npw, const int32_t* g_to_grid_host,
 
 /* apply_batch (init.hpp:59-61; serial.hpp:110-155): hpsi = H psi for nvec
  * vectors, device pointers, FP64 in and out.  precision Q3B_MIXED runs the
- * transforms and projector products in FP32 (inputs rounded, outputs widened). */
+ * transforms and projector products in FP32 (inputs rounded, outputs widened).
+ * Asynchronous: the work is queued on the context's stream (q3b_get_stream)
+ * and the call returns; psi must be ready on that stream, and hpsi is ready
+ * after q3b_synchronize or an event recorded on it (the reference's GPU form
+ * synchronises the device instead, gpu.hpp:305). */
 int q3b_apply_h(q3b_context* ctx, const q3b_cplx128* psi_dev, q3b_cplx128* hpsi_dev, int nvec,
                 int precision);
 
@@ -266,6 +270,30 @@ int q3b_hegv(q3b_context* ctx, int n, const q3b_cplx128* h_dev, const q3b_cplx12
  * captured the third time the same problem shape meets the same buffers and
  * replayed after that.  No counterpart in the reference (diagnostics). */
 int q3b_graph_stats(q3b_context* ctx, int* captures, int* replays);
+
+/* ---- projector set built on the device (ProjectorSetBuilder) ---------------- */
+
+/* q3b_prepare_kpoint with the Kleinman-Bylander projector matrix built on the
+ * device instead of passed in (compute_kleinman_bylander_projectors,
+ * pseudopotential/planewave/internal/projector.hpp:42-199; device builder
+ * projector_set_builder_gpu.hpp):
+ *   beta_{a,i,m}(G) = Omega^{-1/2} (-i)^l f_i(|k+G|) Y_lm(k+G) exp(-i (k+G).r_a),
+ * f_i by 4-point Lagrange interpolation of a uniform table (q = 0, dq, 2dq,
+ * ...), Y_lm real with the Condon-Shortley phase, projectors atom by atom,
+ * beta by beta, m = 0, 1, -1, 2, -2, ....  Units: kpg_cart (npw x 3, k+G per
+ * plane wave, x y z) in bohr^-1, positions (natoms x 3) in bohr, the volume
+ * in bohr^3, dq in bohr^-1.  Species s has nbeta_of_species[s] beta functions;
+ * beta_l and beta_tables (nq values each) list them species by species.
+ * d_blocks: per-atom D blocks in the projector order above (Ry), as for
+ * q3b_prepare_kpoint.  l <= 4. */
+int q3b_prepare_kpoint_build(q3b_context* ctx, int npw, const int32_t* g_to_grid, const double* ke,
+                             const double* kpg_cart, double cell_volume, int natoms, const double* positions,
+                             const int32_t* species_of_atom, int nspecies, const int32_t* nbeta_of_species,
+                             const int32_t* beta_l, int nq, double dq, const double* beta_tables,
+                             const double* d_blocks);
+/* The projector matrix (npw x P, column-major) the context holds for its
+ * prepared k-point, copied to device memory `beta_dev`; P to *nproj. */
+int q3b_get_projectors(q3b_context* ctx, q3b_cplx128* beta_dev, int* nproj);
 
 /* ---- charge density (PlanewaveChargeDensityAccumulator) --------------------- */
 

@@ -8,6 +8,7 @@ numpy arrays.  Nothing here computes H|psi> itself.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 from typing import Optional
 
@@ -53,6 +54,22 @@ class Context:
 
     def synchronize(self) -> None:
         check(self.handle, self.lib.q3b_synchronize(self.handle))
+
+    @contextlib.contextmanager
+    def ordered_with_torch(self):
+        """Order the library's stream with torch's current stream on this
+        device: work issued inside the block starts after what torch has queued
+        (the inputs it wrote), and torch's later work waits for it (the outputs).
+        No host synchronisation."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        ours = torch.cuda.ExternalStream(self.stream, device=dev)
+        theirs = torch.cuda.current_stream(dev)
+        ours.wait_stream(theirs)
+        try:
+            yield
+        finally:
+            theirs.wait_stream(ours)
 
     def device_bytes(self) -> int:
         return int(self.lib.q3b_device_bytes(self.handle))
@@ -134,12 +151,52 @@ class PlanewaveHamiltonianApplicator:
         if psi.dtype == torch.complex64:
             if hpsi.dtype != torch.complex64:
                 raise ValueError("FP32 input needs an FP32 output")
-            rc = self.lib.q3b_apply_h_f32(self.h, psi.data_ptr(), hpsi.data_ptr(), n)
+            with self.ctx.ordered_with_torch():
+                rc = self.lib.q3b_apply_h_f32(self.h, psi.data_ptr(), hpsi.data_ptr(), n)
         elif psi.dtype == torch.complex128 and hpsi.dtype == torch.complex128:
-            rc = self.lib.q3b_apply_h(self.h, psi.data_ptr(), hpsi.data_ptr(), n, int(precision))
+            with self.ctx.ordered_with_torch():
+                rc = self.lib.q3b_apply_h(self.h, psi.data_ptr(), hpsi.data_ptr(), n, int(precision))
         else:
             raise ValueError("vectors must be complex128 (or complex64 for the FP32 entry)")
         check(self.h, rc)
+
+    def prepare_kpoint_build(self, kpoint_index: int, number_of_plane_waves: int, g_vector_to_grid: np.ndarray,
+                             kinetic_energy_squared: np.ndarray, k_plus_g: np.ndarray, cell_volume: float,
+                             positions: np.ndarray, species_of_atom: np.ndarray, beta_l, beta_tables: np.ndarray,
+                             dq: float, d_blocks: np.ndarray) -> None:
+        """prepare_kpoint with the projector set built on the device from the
+        species' beta-function tables (ProjectorSetBuilder).  k_plus_g: npw x 3
+        (bohr^-1); positions: natoms x 3 (bohr); beta_l: list per species of the
+        l of each beta; beta_tables: (total betas) x nq, species by species."""
+        npw = int(number_of_plane_waves)
+        g2g = np.ascontiguousarray(g_vector_to_grid, dtype=np.int32)
+        ke = np.ascontiguousarray(kinetic_energy_squared, dtype=np.float64)
+        kpg = np.ascontiguousarray(k_plus_g, dtype=np.float64)
+        pos = np.ascontiguousarray(positions, dtype=np.float64)
+        spec = np.ascontiguousarray(species_of_atom, dtype=np.int32)
+        nb = np.array([len(x) for x in beta_l], dtype=np.int32)
+        ls = np.array([l for x in beta_l for l in x], dtype=np.int32)
+        tab = np.ascontiguousarray(beta_tables, dtype=np.float64)
+        dblk = np.ascontiguousarray(d_blocks, dtype=np.float64)
+        nq = int(tab.shape[1]) if tab.ndim == 2 else 0
+        check(self.h, self.lib.q3b_prepare_kpoint_build(
+            self.h, npw, _ptr(g2g), _ptr(ke), _ptr(kpg), float(cell_volume), int(pos.shape[0]), _ptr(pos),
+            _ptr(spec), int(nb.size), _ptr(nb), _ptr(ls), nq, float(dq), _ptr(tab), _ptr(dblk)))
+        self.npw = npw
+        self.kpoint_index = kpoint_index
+
+    def projectors(self):
+        """The prepared k-point's projector matrix as a CUDA tensor (P x npw)."""
+        import ctypes as C
+        import torch
+        n = C.c_int()
+        check(self.h, self.lib.q3b_get_projectors(self.h, None, C.byref(n)))
+        out = torch.empty((n.value, self.npw), dtype=torch.complex128, device=torch.device("cuda", self.ctx.device))
+        if n.value:
+            with self.ctx.ordered_with_torch():
+                rc = self.lib.q3b_get_projectors(self.h, out.data_ptr(), C.byref(n))
+            check(self.h, rc)
+        return out
 
     def accumulate_density(self, bands, weights: np.ndarray, rho) -> None:
         """PlanewaveChargeDensityAccumulator at this k-point: rho += sum_b w_b |psi_b(r)|^2.
@@ -148,8 +205,9 @@ class PlanewaveHamiltonianApplicator:
         (k-point weight x occupation / cell volume; 0 skips a band); rho: float64
         CUDA tensor of N1*N2*N3 values, natural grid order, added to."""
         w = np.ascontiguousarray(weights, dtype=np.float64)
-        check(self.h, self.lib.q3b_accumulate_density(self.h, bands.data_ptr(), int(w.size), _ptr(w),
-                                                      rho.data_ptr()))
+        with self.ctx.ordered_with_torch():
+            rc = self.lib.q3b_accumulate_density(self.h, bands.data_ptr(), int(w.size), _ptr(w), rho.data_ptr())
+        check(self.h, rc)
 
     def apply_batch_host(self, psi: np.ndarray, number_of_vectors: int,
                          precision: int = FP64) -> np.ndarray:

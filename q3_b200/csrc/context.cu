@@ -284,7 +284,7 @@ void Context::build_plan() {
 }
 
 void Context::prepare_kpoint(int npw, const int32_t* g2g, const double* ke, const double2* beta,
-                             int nproj, int natoms, const int32_t* offs, const double* dblk) {
+                             int nproj, int natoms, const int32_t* offs, const double* dblk, bool beta_on_device) {
     if (!pot_valid && n1 == 0) throw Status(Q3B_ERR_STATE, "call q3b_set_potential before q3b_prepare_kpoint");
     if (npw <= 0 || !g2g || !ke) throw Status(Q3B_ERR_INVALID, "bad plane-wave list");
     if (nproj < 0 || (nproj > 0 && (!beta || natoms <= 0 || !offs || !dblk)))
@@ -301,10 +301,17 @@ void Context::prepare_kpoint(int npw, const int32_t* g2g, const double* ke, cons
     if (nproj > 0) {
         if (offs[0] != 0 || offs[natoms] != nproj) throw Status(Q3B_ERR_INVALID, "atom offsets do not cover the projectors");
         const size_t nb = (size_t)npw * nproj;
-        upload(this, kp.beta64, beta, nb);
-        std::vector<float2> b32(nb);
-        for (size_t i = 0; i < nb; ++i) b32[i] = make_float2((float)beta[i].x, (float)beta[i].y);
-        upload(this, kp.beta32, b32.data(), nb);
+        if (beta_on_device) {
+            kp.beta64.reserve(this, nb * sizeof(double2));
+            kp.beta32.reserve(this, nb * sizeof(float2));
+            Q3B_CUDA(cudaMemcpyAsync(kp.beta64.ptr, beta, nb * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+            convert<double, float>(stream, (long)nb, kp.beta64.as<double2>(), kp.beta32.as<float2>());
+        } else {
+            upload(this, kp.beta64, beta, nb);
+            std::vector<float2> b32(nb);
+            for (size_t i = 0; i < nb; ++i) b32[i] = make_float2((float)beta[i].x, (float)beta[i].y);
+            upload(this, kp.beta32, b32.data(), nb);
+        }
         kp.beta_pk_overlap.reserve(this, tc::packed_a_bytes(nproj, npw));
         kp.beta_pk_accum.reserve(this, tc::packed_a_bytes(npw, nproj));
         tc::pack_a(stream, nproj, npw, kp.beta32.as<float2>(), npw, true, kp.beta_pk_overlap.as<unsigned char>());

@@ -96,7 +96,7 @@ class Context {
 
     void set_potential(const double* v, int a, int b, int c);
     void prepare_kpoint(int npw, const int32_t* g2g, const double* ke, const double2* beta, int nproj,
-                        int natoms, const int32_t* offs, const double* dblk);
+                        int natoms, const int32_t* offs, const double* dblk, bool beta_on_device = false);
     void require_ready() const;
 
     template <typename R> const LocalPlan<R>& local_plan() const;

@@ -80,8 +80,9 @@ class PlanewaveDavidsonDiagonalizer:
                                              C.byref(self.opts), C.byref(st))
             out = x
         else:
-            rc = self.lib.q3b_davidson_solve_dev(h, bands.data_ptr(), eig.ctypes.data, nb,
-                                                 C.byref(self.opts), C.byref(st))
+            with self.ap.ctx.ordered_with_torch():
+                rc = self.lib.q3b_davidson_solve_dev(h, bands.data_ptr(), eig.ctypes.data, nb,
+                                                     C.byref(self.opts), C.byref(st))
             out = bands
         check(h, rc)
         stages = dict(zip(DavidsonStats.STAGES, list(st.stage_ms)))
@@ -99,6 +100,7 @@ def hegv(applicator, h: np.ndarray, s: np.ndarray):
     S = torch.from_numpy(np.ascontiguousarray(np.asarray(s, np.complex128).T)).to(dev)
     w = torch.empty(n, dtype=torch.float64, device=dev)
     Z = torch.empty(n, n, dtype=torch.complex128, device=dev)
-    check(applicator.h, applicator.lib.q3b_hegv(applicator.h, n, H.data_ptr(), S.data_ptr(), n,
-                                                w.data_ptr(), Z.data_ptr()))
+    with applicator.ctx.ordered_with_torch():
+        rc = applicator.lib.q3b_hegv(applicator.h, n, H.data_ptr(), S.data_ptr(), n, w.data_ptr(), Z.data_ptr())
+    check(applicator.h, rc)
     return w.cpu().numpy(), Z.cpu().numpy().T

@@ -39,8 +39,9 @@ class StartingSubspaceSolver:
         c = np.asfortranarray(coefficients[:, :number_of_bands], dtype=np.complex128)
         out = torch.empty((number_of_bands, self.ap.npw), dtype=torch.complex128,
                           device=torch.device("cuda", self.ap.ctx.device))
-        check(self.ap.h, self.lib.q3b_start_rotate(self.ap.h, c.ctypes.data, int(number_of_bands),
-                                                   out.data_ptr()))
+        with self.ap.ctx.ordered_with_torch():
+            rc = self.lib.q3b_start_rotate(self.ap.h, c.ctypes.data, int(number_of_bands), out.data_ptr())
+        check(self.ap.h, rc)
         return out
 
 
@@ -53,7 +54,8 @@ def rotate_starting_vectors(applicator, vectors: np.ndarray, number_of_bands: in
     out = torch.empty((number_of_bands, applicator.npw), dtype=torch.complex128,
                       device=torch.device("cuda", applicator.ctx.device))
     eig = np.empty(number_of_bands, dtype=np.float64)
-    check(applicator.h, applicator.lib.q3b_starting_subspace(applicator.h, chi.ctypes.data, n,
-                                                             int(number_of_bands), out.data_ptr(),
-                                                             eig.ctypes.data))
+    with applicator.ctx.ordered_with_torch():
+        rc = applicator.lib.q3b_starting_subspace(applicator.h, chi.ctypes.data, n, int(number_of_bands),
+                                                  out.data_ptr(), eig.ctypes.data)
+    check(applicator.h, rc)
     return eig, out
