@@ -315,12 +315,11 @@ template <typename R> class Davidson {
         dscratch_.used = 0;
         const int nvec = std::min(nb_, n);
         GemmWorkspace gws = c_.gemm_ws(cgemm_workspace_bytes<double>(n, n, n));
-        const int info = dense::hegv(st_, n, H, S, ld, w_, evec_, nvec, dscratch_, gws, &c_.hegv_graphs);
-        if (info == 0 && publish) {
-            whost_.assign(n, 0.0);
-            Q3B_CUDA(cudaMemcpyAsync(whost_.data(), w_, n * sizeof(double), cudaMemcpyDeviceToHost, st_));
-            Q3B_CUDA(cudaStreamSynchronize(st_));
-        }
+        // the eigenvalues come back in the solve's own status read
+        wread_.resize(n);
+        const int info = dense::hegv(st_, n, H, S, ld, w_, evec_, nvec, dscratch_, gws, &c_.hegv_graphs,
+                                     wread_.data());
+        if (info == 0 && publish) whost_.assign(wread_.begin(), wread_.begin() + n);
         return info;
     }
 
@@ -372,9 +371,8 @@ template <typename R> class Davidson {
         // The next iteration's subspace is the nb Ritz vectors just formed: its
         // matrices are diag(w) and the identity to rounding, so its eigenpairs
         // are these eigenvalues (left in w_[0, nb)) and unit vectors.
-        collapse_w_.assign(nb_, 0.0);
-        Q3B_CUDA(cudaMemcpyAsync(collapse_w_.data(), w_, nb_ * sizeof(double), cudaMemcpyDeviceToHost, st_));
-        Q3B_CUDA(cudaStreamSynchronize(st_));
+        // the collapse's eigenvalues were read back by its subspace solve
+        collapse_w_.assign(wread_.begin(), wread_.begin() + nb_);
         reuse_collapse_ = true;
         return nb_;
     }
@@ -580,6 +578,7 @@ template <typename R> class Davidson {
     dense::Scratch dscratch_;
     std::vector<double> whost_;
     std::vector<double> collapse_w_;
+    std::vector<double> wread_;  // eigenvalues of the last subspace solve, on the host
     bool reuse_collapse_ = false;
 };
 

@@ -967,6 +967,10 @@ HeevPlan heev_plan(int n, int nvec, Scratch& ws) {
     Q3B_CUDA(cudaGetDevice(&device));
     int nsm = 0;
     Q3B_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    static std::once_flag once_inv;
+    std::call_once(once_inv, [] {
+        cudaFuncSetAttribute(tridiag_invit_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvitSmemLimit);
+    });
     // blocks: about 8 columns each, at most one per SM; columns (and W) in shared memory
     p.G = std::max(1, std::min(nsm, (n + 7) / 8));
     p.cpb = (n + p.G - 1) / p.G;
@@ -1118,7 +1122,7 @@ cudaGraphExec_t HegvGraphs::capture(cudaStream_t st, void (*issue)(void*), void*
 }
 
 int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, double* w, double2* Z,
-         int nvec, Scratch& ws, const GemmWorkspace& gws, HegvGraphs* graphs) {
+         int nvec, Scratch& ws, const GemmWorkspace& gws, HegvGraphs* graphs, double* w_host) {
     if (n <= 0) return 0;
     const size_t used0 = ws.used;
     const size_t nn = (size_t)n * n;
@@ -1161,6 +1165,7 @@ int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, dou
     int flags[2] = {0, 0};
     Q3B_CUDA(cudaMemcpyAsync(&flags[0], c.info, sizeof(int), cudaMemcpyDeviceToHost, st));
     Q3B_CUDA(cudaMemcpyAsync(&flags[1], hp.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (w_host) Q3B_CUDA(cudaMemcpyAsync(w_host, w, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
     Q3B_CUDA(cudaStreamSynchronize(st));
     if (flags[1]) throw Status(Q3B_ERR_INTERNAL, "eigensolver grid barrier timed out");
     return flags[0] ? n + flags[0] : 0;

@@ -121,8 +121,11 @@ template <typename F> cudaGraphExec_t HegvGraphs::get(const Key& k, F&& issue) {
 // S-orthonormal eigenvectors in Z (n x nvec, ld n).  Returns 0, or n + j
 // when S is not positive definite (zhegv's convention).  With `graphs`, the
 // launch sequence is replayed from a captured graph when one matches.
+// With w_host, the eigenvalues are also copied to the host in the same
+// synchronisation that reads the status words.
 int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, double* w, double2* Z,
-         int nvec, Scratch& ws, const GemmWorkspace& gws, HegvGraphs* graphs = nullptr);
+         int nvec, Scratch& ws, const GemmWorkspace& gws, HegvGraphs* graphs = nullptr,
+         double* w_host = nullptr);
 
 // Standard Hermitian eigenproblem of a full (both triangles) matrix A (n x n,
 // ld n; read only).  Eigenvalues ascending in w, the first nvec eigenvectors
