@@ -562,26 +562,26 @@ __device__ int g_tc_error;
 }  // namespace
 
 int* error_word() {
-    static int* addr[64] = {};
-    static std::mutex mu;
+    // per host thread: the device it last asked for and the word's address there
+    thread_local int cached_dev = -1;
+    thread_local int* cached = nullptr;
     int dev = 0;
     Q3B_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
-    std::lock_guard<std::mutex> lk(mu);
-    if (!addr[dev]) {
+    if (dev != cached_dev || !cached) {
         void* p = nullptr;
         Q3B_CUDA(cudaGetSymbolAddress(&p, g_tc_error));
-        addr[dev] = static_cast<int*>(p);
+        cached = static_cast<int*>(p);
+        cached_dev = dev;
     }
-    return addr[dev];
+    return cached;
 }
 
 void check_error(cudaStream_t st) {
     int* w = error_word();
-    int h = 0;
-    Q3B_CUDA(cudaMemcpyAsync(&h, w, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int* hb = static_cast<int*>(host_readback(sizeof(int)));
+    Q3B_CUDA(cudaMemcpyAsync(hb, w, sizeof(int), cudaMemcpyDeviceToHost, st));
     Q3B_CUDA(cudaStreamSynchronize(st));
-    if (h) {
+    if (hb[0]) {
         Q3B_CUDA(cudaMemsetAsync(w, 0, sizeof(int), st));
         throw CudaError("tensor-core GEMM: a pipeline wait timed out");
     }

@@ -84,6 +84,22 @@ void count_launch();
         Q3B_CUDA(cudaGetLastError()); \
     } while (0)
 
+// Pinned host memory of the calling host thread, at least `bytes` long, for
+// small device->host reads (status words, eigenvalues, norms).  A read into
+// pageable memory is staged by the driver through memory it shares between
+// threads, and several threads solving at once on their own streams then wait
+// on each other's reads; a pinned destination is written by the copy engine
+// directly.  The block stays valid until the next call from the same thread.
+void* host_readback(size_t bytes);
+
+// Copies `bytes` of host memory to `dst` on `st` through the calling thread's
+// pinned staging block (same reason), for the small uploads inside the solver
+// loop.  The host data is taken at the call; the block is reused only after
+// the stream has consumed the previous copy.  The large one-off copies of a
+// request's setup stay on the driver's pageable path, which pipelines its
+// staging with the transfer (faster there with several threads at once).
+void upload_async(void* dst, const void* src, size_t bytes, cudaStream_t st);
+
 inline int ceil_div(long a, long b) { return static_cast<int>((a + b - 1) / b); }
 
 }  // namespace q3b

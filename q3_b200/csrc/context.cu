@@ -1,4 +1,5 @@
 // q3b context: HBM accounting, potential, k-point plan, H|psi> orchestration.
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -11,6 +12,71 @@
 #include "q3b.h"
 
 namespace q3b {
+
+// ------------------------------------------------------------ host readback
+namespace {
+struct PinnedBlock {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    ~PinnedBlock() {
+        if (ptr) cudaFreeHost(ptr);
+    }
+};
+}  // namespace
+
+void* host_readback(size_t bytes) {
+    thread_local PinnedBlock blk;
+    if (bytes > blk.bytes || !blk.ptr) {
+        const size_t want = std::max<size_t>(bytes, 64 << 10);
+        if (blk.ptr) Q3B_CUDA(cudaFreeHost(blk.ptr));
+        blk.ptr = nullptr;
+        blk.bytes = 0;
+        Q3B_CUDA(cudaHostAlloc(&blk.ptr, want, cudaHostAllocDefault));
+        blk.bytes = want;
+    }
+    return blk.ptr;
+}
+
+namespace {
+struct StagingBlock {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t consumed = nullptr;
+    bool pending = false;
+    ~StagingBlock() {
+        if (pending) cudaEventSynchronize(consumed);
+        if (ptr) cudaFreeHost(ptr);
+        if (consumed) cudaEventDestroy(consumed);
+    }
+};
+}  // namespace
+
+// the staging block stays at most this large; longer copies go in pieces
+constexpr size_t kStagingChunk = 4u << 20;
+
+void upload_async(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    if (bytes == 0) return;
+    thread_local StagingBlock blk;
+    if (!blk.consumed) Q3B_CUDA(cudaEventCreateWithFlags(&blk.consumed, cudaEventDisableTiming));
+    const size_t chunk = std::min(bytes, kStagingChunk);
+    for (size_t off = 0; off < bytes; off += chunk) {
+        const size_t len = std::min(chunk, bytes - off);
+        if (blk.pending) Q3B_CUDA(cudaEventSynchronize(blk.consumed));
+        blk.pending = false;
+        if (len > blk.bytes || !blk.ptr) {
+            const size_t want = std::max<size_t>(len, 64 << 10);
+            if (blk.ptr) Q3B_CUDA(cudaFreeHost(blk.ptr));
+            blk.ptr = nullptr;
+            blk.bytes = 0;
+            Q3B_CUDA(cudaHostAlloc(&blk.ptr, want, cudaHostAllocDefault));
+            blk.bytes = want;
+        }
+        std::memcpy(blk.ptr, static_cast<const char*>(src) + off, len);
+        Q3B_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + off, blk.ptr, len, cudaMemcpyHostToDevice, st));
+        Q3B_CUDA(cudaEventRecord(blk.consumed, st));
+        blk.pending = true;
+    }
+}
 
 // ------------------------------------------------------------------ DevBuf
 DevBuf::~DevBuf() { release(); }

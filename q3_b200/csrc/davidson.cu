@@ -277,9 +277,10 @@ template <typename R> class Davidson {
             }
             column_norms<R><<<1, 256, 0, st_>>>(npw_, v, norms_);
             Q3B_LAUNCH_CHECK();
-            double nrm = 0.0;
-            Q3B_CUDA(cudaMemcpyAsync(&nrm, norms_, sizeof(double), cudaMemcpyDeviceToHost, st_));
+            double* hb = static_cast<double*>(host_readback(sizeof(double)));
+            Q3B_CUDA(cudaMemcpyAsync(hb, norms_, sizeof(double), cudaMemcpyDeviceToHost, st_));
             Q3B_CUDA(cudaStreamSynchronize(st_));
+            const double nrm = hb[0];
             const double n2 = nrm * nrm;
             if (n2 > kNormThreshold) {
                 scale_vector<R><<<grid_for(npw_), 256, 0, st_>>>(npw_, v, 1.0 / nrm);
@@ -327,7 +328,7 @@ template <typename R> class Davidson {
     int corrections(int basis, const std::vector<int>& bands, int maxcand) {
         int ncand = std::min<int>(static_cast<int>(bands.size()), maxcand);
         if (ncand <= 0) return 0;
-        Q3B_CUDA(cudaMemcpyAsync(idx_, bands.data(), ncand * sizeof(int), cudaMemcpyHostToDevice, st_));
+        upload_async(idx_, bands.data(), ncand * sizeof(int), st_);
         pack_coefficients<R><<<grid_for((long)basis * ncand), 256, 0, st_>>>(basis, ncand, evec_, idx_, w_,
                                                                              cpack_, cneg_, eps_);
         Q3B_LAUNCH_CHECK();
@@ -384,7 +385,7 @@ template <typename R> class Davidson {
         if (resid_max) {
             std::vector<int> all(nb_);
             std::iota(all.begin(), all.end(), 0);
-            Q3B_CUDA(cudaMemcpyAsync(idx_, all.data(), nb_ * sizeof(int), cudaMemcpyHostToDevice, st_));
+            upload_async(idx_, all.data(), nb_ * sizeof(int), st_);
             pack_coefficients<R><<<grid_for((long)basis * nb_), 256, 0, st_>>>(basis, nb_, evec_, idx_, w_,
                                                                                cpack_, cneg_, eps_);
             Q3B_LAUNCH_CHECK();
@@ -392,10 +393,10 @@ template <typename R> class Davidson {
             gemm(false, npw_, nb_, basis, one(), HV_, npw_, cpack_, basis, one(), tmp_, npw_);
             column_norms<R><<<nb_, 256, 0, st_>>>(npw_, tmp_, norms_);
             Q3B_LAUNCH_CHECK();
-            std::vector<double> h(nb_);
-            Q3B_CUDA(cudaMemcpyAsync(h.data(), norms_, nb_ * sizeof(double), cudaMemcpyDeviceToHost, st_));
+            double* h = static_cast<double*>(host_readback(nb_ * sizeof(double)));
+            Q3B_CUDA(cudaMemcpyAsync(h, norms_, nb_ * sizeof(double), cudaMemcpyDeviceToHost, st_));
             Q3B_CUDA(cudaStreamSynchronize(st_));
-            *resid_max = *std::max_element(h.begin(), h.end());
+            *resid_max = *std::max_element(h, h + nb_);
         }
     }
 
@@ -406,8 +407,8 @@ template <typename R> class Davidson {
     }
 
     std::vector<double> subspace_diagonal(int n) {
-        std::vector<double2> d(n);
-        Q3B_CUDA(cudaMemcpy2DAsync(d.data(), sizeof(double2), Hs_, (maxn_ + 1) * sizeof(double2),
+        double2* d = static_cast<double2*>(host_readback(n * sizeof(double2)));
+        Q3B_CUDA(cudaMemcpy2DAsync(d, sizeof(double2), Hs_, (maxn_ + 1) * sizeof(double2),
                                    sizeof(double2), n, cudaMemcpyDeviceToHost, st_));
         Q3B_CUDA(cudaStreamSynchronize(st_));
         std::vector<double> r(n);
@@ -445,7 +446,7 @@ template <typename R> class Davidson {
             std::vector<int> gsel;
             for (int band = start; band < nb_; ++band) gsel.push_back(order[band]);
             const int ncand = static_cast<int>(gsel.size());
-            Q3B_CUDA(cudaMemcpyAsync(idx_, gsel.data(), ncand * sizeof(int), cudaMemcpyHostToDevice, st_));
+            upload_async(idx_, gsel.data(), ncand * sizeof(int), st_);
             unit_vectors<R><<<grid_for((long)npw_ * ncand), 256, 0, st_>>>(npw_, ncand, idx_,
                                                                            V_ + (size_t)basis * npw_);
             Q3B_LAUNCH_CHECK();

@@ -15,6 +15,7 @@
 //         division-free Sturm counts (one warp per eigenvalue), eigenvectors
 //         by inverse iteration in shared memory with Gram-Schmidt inside
 //         clusters of close eigenvalues, then Z = Q (phase * Y) by GEMM.
+#include <cstring>
 #include <algorithm>
 #include <cmath>
 #include <mutex>
@@ -872,10 +873,10 @@ void potrf_launch(cudaStream_t st, int n, double2* A, int lda, const Chol& c) {
 
 int potrf_impl(cudaStream_t st, int n, double2* A, int lda, const Chol& c) {
     potrf_launch(st, n, A, lda, c);
-    int info = 0;
-    Q3B_CUDA(cudaMemcpyAsync(&info, c.info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int* hb = static_cast<int*>(host_readback(sizeof(int)));
+    Q3B_CUDA(cudaMemcpyAsync(hb, c.info, sizeof(int), cudaMemcpyDeviceToHost, st));
     Q3B_CUDA(cudaStreamSynchronize(st));
-    return info;
+    return hb[0];
 }
 
 void trtri_impl(cudaStream_t st, int n, const double2* A, int lda, const Chol& c, double2* Ui) {
@@ -1042,10 +1043,10 @@ void heev_launch(cudaStream_t st, const HeevPlan& p, const double2* A, double* w
 }
 
 int read_flag(cudaStream_t st, const int* flag) {
-    int h = 0;
-    Q3B_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int* hb = static_cast<int*>(host_readback(sizeof(int)));
+    Q3B_CUDA(cudaMemcpyAsync(hb, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
     Q3B_CUDA(cudaStreamSynchronize(st));
-    return h;
+    return hb[0];
 }
 
 }  // namespace
@@ -1162,11 +1163,15 @@ int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, dou
     }
     // a failed Cholesky leaves the later steps on garbage: their result is
     // discarded, and every loop in them is bounded
-    int flags[2] = {0, 0};
+    // status words and eigenvalues read back together, one synchronisation
+    char* hb = static_cast<char*>(host_readback(2 * sizeof(double) + (w_host ? (size_t)n * sizeof(double) : 0)));
+    int* flags = reinterpret_cast<int*>(hb);
+    double* wb = reinterpret_cast<double*>(hb + 2 * sizeof(double));
     Q3B_CUDA(cudaMemcpyAsync(&flags[0], c.info, sizeof(int), cudaMemcpyDeviceToHost, st));
     Q3B_CUDA(cudaMemcpyAsync(&flags[1], hp.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    if (w_host) Q3B_CUDA(cudaMemcpyAsync(w_host, w, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (w_host) Q3B_CUDA(cudaMemcpyAsync(wb, w, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
     Q3B_CUDA(cudaStreamSynchronize(st));
+    if (w_host) std::memcpy(w_host, wb, (size_t)n * sizeof(double));
     if (flags[1]) throw Status(Q3B_ERR_INTERNAL, "eigensolver grid barrier timed out");
     return flags[0] ? n + flags[0] : 0;
 }
