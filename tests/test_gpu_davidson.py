@@ -55,7 +55,7 @@ def test_hegv_48_generalized(cuda_device, ctx_app):
     assert np.max(np.abs(z.conj().T @ s @ z - np.eye(48))) < 1e-10
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 31, 32, 33, 96, 200, 512])
+@pytest.mark.parametrize("n", [1, 2, 3, 16, 17, 31, 32, 33, 64, 65, 96, 128, 129, 200, 255, 256, 257, 512])
 def test_hegv_random(cuda_device, ctx_app, n):
     from q3_b200.davidson import hegv
     rng = np.random.default_rng(n)
