@@ -15,33 +15,35 @@ template <typename R> struct GemmTile;
 template <> struct GemmTile<double> { static constexpr int BK = 8; };
 template <> struct GemmTile<float> { static constexpr int BK = 16; };
 
-// One 64x64 tile of C per block, 4x4 complex outputs per thread.  With
-// kchunk < K the block handles K range [z*kchunk, (z+1)*kchunk) and writes its
-// raw sum to part[z] (ld M); otherwise it applies alpha/beta into C.
-template <typename R, bool CONJ_A>
+// One BM x BN tile of C per block (64x64, or 32x32 for small products),
+// (BM/16) x (BN/16) complex outputs per thread.  With kchunk < K the block
+// handles K range [z*kchunk, (z+1)*kchunk) and writes its raw sum to part[z]
+// (ld M); otherwise it applies alpha/beta into C.
+template <typename R, bool CONJ_A, int BM = kBM, int BN = kBN>
 __global__ void __launch_bounds__(kThreads)
 cgemm_kernel(int M, int N, int K, cplx_t<R> alpha, const cplx_t<R>* __restrict__ A, long lda,
              const cplx_t<R>* __restrict__ B, long ldb, cplx_t<R> beta, cplx_t<R>* C, long ldc,
              int kchunk, cplx_t<R>* part) {
     using T = cplx_t<R>;
     constexpr int BK = GemmTile<R>::BK;
-    constexpr int LA = (BK * kBM) / kThreads;  // complex loads per thread, A tile
-    constexpr int LB = (BK * kBN) / kThreads;
-    __shared__ T As[2][BK][kBM + 1];
-    __shared__ T Bs[2][BK][kBN + 1];
+    constexpr int TM = BM / 16, TN = BN / 16;  // outputs per thread
+    constexpr int LA = (BK * BM + kThreads - 1) / kThreads;  // complex loads per thread, A tile
+    constexpr int LB = (BK * BN + kThreads - 1) / kThreads;
+    __shared__ T As[2][BK][BM + 1];
+    __shared__ T Bs[2][BK][BN + 1];
 
     const int tid = threadIdx.x;
     const int tx = tid % 16, ty = tid / 16;
     // N tiles run fastest: the blocks that share an A tile run together
-    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int kbeg = blockIdx.z * kchunk;
     const int kend = min(K, kbeg + kchunk);
 
-    T acc[4][4];
+    T acc[TM][TN];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = czero<T>();
+        for (int j = 0; j < TN; ++j) acc[i][j] = czero<T>();
 
     T ra[LA], rb[LB];
     auto load = [&](int k0) {
@@ -53,12 +55,12 @@ cgemm_kernel(int M, int N, int K, cplx_t<R> alpha, const cplx_t<R>* __restrict__
                 k = idx % BK;
                 m = idx / BK;
             } else {
-                m = idx % kBM;
-                k = idx / kBM;
+                m = idx % BM;
+                k = idx / BM;
             }
             const int gk = k0 + k, gm = m0 + m;
             T v = czero<T>();
-            if (gk < kend && gm < M) {
+            if (idx < BK * BM && gk < kend && gm < M) {
                 v = CONJ_A ? conj2(A[gk + (long)gm * lda]) : A[gm + (long)gk * lda];
             }
             ra[r] = v;
@@ -68,26 +70,28 @@ cgemm_kernel(int M, int N, int K, cplx_t<R> alpha, const cplx_t<R>* __restrict__
             const int idx = tid + r * kThreads;
             const int k = idx % BK, n = idx / BK;
             const int gk = k0 + k, gn = n0 + n;
-            rb[r] = (gk < kend && gn < N) ? B[gk + (long)gn * ldb] : czero<T>();
+            rb[r] = (idx < BK * BN && gk < kend && gn < N) ? B[gk + (long)gn * ldb] : czero<T>();
         }
     };
     auto store = [&](int buf) {
 #pragma unroll
         for (int r = 0; r < LA; ++r) {
             const int idx = tid + r * kThreads;
+            if (idx >= BK * BM) continue;
             int k, m;
             if (CONJ_A) {
                 k = idx % BK;
                 m = idx / BK;
             } else {
-                m = idx % kBM;
-                k = idx / kBM;
+                m = idx % BM;
+                k = idx / BM;
             }
             As[buf][k][m] = ra[r];
         }
 #pragma unroll
         for (int r = 0; r < LB; ++r) {
             const int idx = tid + r * kThreads;
+            if (idx >= BK * BN) continue;
             Bs[buf][idx % BK][idx / BK] = rb[r];
         }
     };
@@ -103,15 +107,15 @@ cgemm_kernel(int M, int N, int K, cplx_t<R> alpha, const cplx_t<R>* __restrict__
         if (more) load(k0 + BK);
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
-            T a[4], b[4];
+            T a[TM], b[TN];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][ty + 16 * i];
+            for (int i = 0; i < TM; ++i) a[i] = As[buf][kk][ty + 16 * i];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk][tx + 16 * j];
+            for (int j = 0; j < TN; ++j) b[j] = Bs[buf][kk][tx + 16 * j];
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < TM; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) cfma(acc[i][j], a[i], b[j]);
+                for (int j = 0; j < TN; ++j) cfma(acc[i][j], a[i], b[j]);
         }
         if (more) store(buf ^ 1);
         __syncthreads();
@@ -120,11 +124,11 @@ cgemm_kernel(int M, int N, int K, cplx_t<R> alpha, const cplx_t<R>* __restrict__
 
     const bool use_beta = (beta.x != R(0) || beta.y != R(0));
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < TM; ++i) {
         const int gm = m0 + ty + 16 * i;
         if (gm >= M) continue;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < TN; ++j) {
             const int gn = n0 + tx + 16 * j;
             if (gn >= N) continue;
             if (part) {
@@ -159,8 +163,15 @@ __global__ void splitk_reduce(int M, int N, int splits, const cplx_t<R>* __restr
     }
 }
 
-template <typename R> int choose_splits(int M, int N, int K) {
-    const int tiles = ceil_div(M, kBM) * ceil_div(N, kBN);
+// Products whose 64x64 tiling leaves most SMs idle (the subspace eigensolver's
+// n x n x n products, n <= 256) run on 32x32 tiles: four times the blocks and
+// a quarter of the serial K loop per block.
+constexpr long kSmallTiles = 64;
+inline bool small_tiles(int M, int N) { return (long)ceil_div(M, kBM) * ceil_div(N, kBN) < kSmallTiles; }
+
+// K splits for a product with `tiles` output tiles (never more than for
+// 64x64 tiles, which size the workspace)
+inline int choose_splits_for(int tiles, int K) {
     const int target = 2 * 148;
     int s = ceil_div(target, tiles);
     const int kmax = ceil_div(K, 128);
@@ -168,6 +179,10 @@ template <typename R> int choose_splits(int M, int N, int K) {
     if (s < 1) s = 1;
     if (s > 64) s = 64;
     return s;
+}
+
+template <typename R> int choose_splits(int M, int N, int K) {
+    return choose_splits_for(ceil_div(M, kBM) * ceil_div(N, kBN), K);
 }
 
 }  // namespace
@@ -204,7 +219,9 @@ void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, cplx_t<R> alpha, c
         Q3B_LAUNCH_CHECK();
         return;
     }
-    int splits = conj_a ? choose_splits<R>(M, N, K) : 1;
+    const bool small = small_tiles(M, N);
+    const int bm = small ? 32 : kBM;
+    int splits = conj_a ? choose_splits_for(ceil_div(M, bm) * ceil_div(N, bm), K) : 1;
     size_t need = (size_t)splits * M * N * sizeof(T);
     if (splits > 1 && (ws.ptr == nullptr || ws.bytes < need)) splits = 1;
     int kchunk = K;
@@ -213,15 +230,23 @@ void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, cplx_t<R> alpha, c
         kchunk = ceil_div(kchunk, BK) * BK;
         splits = ceil_div(K, kchunk);
     }
-    if (ceil_div(M, kBM) > 65535) throw std::runtime_error("complex GEMM: M too large");
-    dim3 grid(ceil_div(N, kBN), ceil_div(M, kBM), splits);
+    if (ceil_div(M, bm) > 65535) throw std::runtime_error("complex GEMM: M too large");
+    dim3 grid(ceil_div(N, bm), ceil_div(M, bm), splits);
     T* part = splits > 1 ? static_cast<T*>(ws.ptr) : nullptr;
-    if (conj_a)
+    if (small) {
+        if (conj_a)
+            cgemm_kernel<R, true, 32, 32><<<grid, kThreads, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta,
+                                                                    C, ldc, kchunk, part);
+        else
+            cgemm_kernel<R, false, 32, 32><<<grid, kThreads, 0, st>>>(M, N, K, alpha, A, lda, B, ldb,
+                                                                     beta, C, ldc, kchunk, part);
+    } else if (conj_a) {
         cgemm_kernel<R, true><<<grid, kThreads, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
                                                          ldc, kchunk, part);
-    else
+    } else {
         cgemm_kernel<R, false><<<grid, kThreads, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C,
                                                           ldc, kchunk, part);
+    }
     Q3B_LAUNCH_CHECK();
     if (splits > 1) {
         const long total = (long)M * N;

@@ -316,11 +316,11 @@ template <typename R> class Davidson {
         dscratch_.used = 0;
         const int nvec = std::min(nb_, n);
         GemmWorkspace gws = c_.gemm_ws(cgemm_workspace_bytes<double>(n, n, n));
-        // the eigenvalues come back in the solve's own status read
-        wread_.resize(n);
+        // the lowest nvec eigenvalues come back in the solve's own status read
+        wread_.assign(n, 0.0);
         const int info = dense::hegv(st_, n, H, S, ld, w_, evec_, nvec, dscratch_, gws, &c_.hegv_graphs,
                                      wread_.data());
-        if (info == 0 && publish) whost_.assign(wread_.begin(), wread_.begin() + n);
+        if (info == 0 && publish) whost_.assign(wread_.begin(), wread_.begin() + nvec);
         return info;
     }
 

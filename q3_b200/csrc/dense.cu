@@ -62,10 +62,12 @@ __device__ __forceinline__ void pivot_terms(double piv, int j, int bs, int r0, d
         if (j < bs) atomicMin(bad, r0 + j + 1);
         piv = 1.0;
     }
-    const double q = sqrt(piv);
-    rp[j] = 1.0 / piv;
-    sq[j] = q;
-    isq[j] = 1.0 / q;
+    // one reciprocal square root on the step's critical path instead of a
+    // square root and two divisions
+    const double iq = rsqrt(piv);
+    rp[j] = iq * iq;
+    sq[j] = piv * iq;
+    isq[j] = iq;
 }
 
 __global__ void __launch_bounds__(1024, 1)
@@ -587,6 +589,7 @@ __device__ __forceinline__ void sturm_counts(int n, const double* d, const doubl
         if (fabs(p[s]) < pivmin) p[s] = -pivmin;
         c[s] = p[s] < 0.0;
     }
+#pragma unroll 4
     for (int k = 1; k < n; ++k) {
         const double dk = d[k], ek = e2[k - 1];
 #pragma unroll
@@ -601,13 +604,27 @@ __device__ __forceinline__ void sturm_counts(int n, const double* d, const doubl
     }
 }
 
-// one warp per eigenvalue: multisection of [lo, hi] on Sturm counts at
-// 32 x kShifts interior points per round (the interval shrinks 65-fold)
+// one warp per eigenvalue (the lowest nw): multisection of [lo, hi] on Sturm
+// counts at 32 x kShifts interior points per round (the interval shrinks
+// 65-fold).  The block stages d and e^2 in shared memory when they fit
+// (kSturmSmemOrder), so the count's loads do not wait on L1 or L2.
 constexpr int kShifts = 2;
-__global__ void tridiag_multisect(int n, const double* d, const double* e2, const double* bounds, double* w) {
+constexpr int kSturmSmemOrder = 3072;
+__global__ void tridiag_multisect(int n, const double* d, const double* e2, const double* bounds, double* w,
+                                  int nw) {
+    extern __shared__ double sturm_smem[];
+    if (n <= kSturmSmemOrder) {
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            sturm_smem[k] = d[k];
+            sturm_smem[n + k] = e2[k];
+        }
+        __syncthreads();
+        d = sturm_smem;
+        e2 = sturm_smem + n;
+    }
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= n) return;
+    if (i >= nw) return;
     constexpr int P = 32 * kShifts;  // points per round
     double a = bounds[0], b = bounds[1];
     const double scale = bounds[2];
@@ -790,6 +807,7 @@ __global__ void tridiag_invit_smem(int n, const double* d, const double* ea, con
         double ys = 1.0;  // pending normalisation of y
         for (int iter = 0; iter < 3; ++iter) {
             double ycur = y[AT(0)] * ys;
+#pragma unroll 4
             for (int t = 0; t + 1 < n; ++t) {
                 const double ynext = y[AT(t + 1)] * ys;
                 const double f = DL[AT(t)];
@@ -804,6 +822,7 @@ __global__ void tridiag_invit_smem(int n, const double* d, const double* ea, con
             double y1 = ycur * DI[AT(n - 1)], y2 = 0.0;
             y[AT(n - 1)] = y1;
             double nr = y1 * y1;
+#pragma unroll 4
             for (int t = n - 2; t >= 0; --t) {
                 const double v = (y[AT(t)] - DU[AT(t)] * y1 - DU2[AT(t)] * y2) * DI[AT(t)];
                 y[AT(t)] = v;
@@ -1024,7 +1043,9 @@ void heev_launch(cudaStream_t st, const HeevPlan& p, const double2* A, double* w
     }
     tridiag_prep<<<1, 32, 0, st>>>(n, p.d, p.e, p.ea, p.e2, p.phase, p.bounds);
     Q3B_LAUNCH_CHECK();
-    tridiag_multisect<<<ceil_div((long)n * 32, 256), 256, 0, st>>>(n, p.d, p.e2, p.bounds, w);
+    const int nw = nvec > 0 ? nvec : n;
+    const size_t sturm_smem = n <= kSturmSmemOrder ? 2 * (size_t)n * sizeof(double) : 0;
+    tridiag_multisect<<<ceil_div((long)nw * 32, 256), 256, sturm_smem, st>>>(n, p.d, p.e2, p.bounds, w, nw);
     Q3B_LAUNCH_CHECK();
     if (nvec > 0) {
         const int T = static_cast<int>(std::min<size_t>(64, kInvitSmemLimit / ((size_t)n * kInvitBytesPerRow)));
@@ -1164,14 +1185,15 @@ int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, dou
     // a failed Cholesky leaves the later steps on garbage: their result is
     // discarded, and every loop in them is bounded
     // status words and eigenvalues read back together, one synchronisation
-    char* hb = static_cast<char*>(host_readback(2 * sizeof(double) + (w_host ? (size_t)n * sizeof(double) : 0)));
+    const size_t nw = nvec > 0 ? nvec : n;
+    char* hb = static_cast<char*>(host_readback(2 * sizeof(double) + (w_host ? nw * sizeof(double) : 0)));
     int* flags = reinterpret_cast<int*>(hb);
     double* wb = reinterpret_cast<double*>(hb + 2 * sizeof(double));
     Q3B_CUDA(cudaMemcpyAsync(&flags[0], c.info, sizeof(int), cudaMemcpyDeviceToHost, st));
     Q3B_CUDA(cudaMemcpyAsync(&flags[1], hp.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    if (w_host) Q3B_CUDA(cudaMemcpyAsync(wb, w, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (w_host) Q3B_CUDA(cudaMemcpyAsync(wb, w, nw * sizeof(double), cudaMemcpyDeviceToHost, st));
     Q3B_CUDA(cudaStreamSynchronize(st));
-    if (w_host) std::memcpy(w_host, wb, (size_t)n * sizeof(double));
+    if (w_host) std::memcpy(w_host, wb, nw * sizeof(double));
     if (flags[1]) throw Status(Q3B_ERR_INTERNAL, "eigensolver grid barrier timed out");
     return flags[0] ? n + flags[0] : 0;
 }

@@ -117,8 +117,8 @@ template <typename F> cudaGraphExec_t HegvGraphs::get(const Key& k, F&& issue) {
 }
 
 // Generalized Hermitian eigenproblem H c = w S c (itype 1; upper triangles of
-// H and S, ld ld).  Eigenvalues ascending in w (n, device), the first nvec
-// S-orthonormal eigenvectors in Z (n x nvec, ld n).  Returns 0, or n + j
+// H and S, ld ld).  The lowest nvec eigenvalues ascending in w (device; all n
+// when nvec is 0), their S-orthonormal eigenvectors in Z (n x nvec, ld n).  Returns 0, or n + j
 // when S is not positive definite (zhegv's convention).  With `graphs`, the
 // launch sequence is replayed from a captured graph when one matches.
 // With w_host, the eigenvalues are also copied to the host in the same
@@ -128,8 +128,8 @@ int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, dou
          double* w_host = nullptr);
 
 // Standard Hermitian eigenproblem of a full (both triangles) matrix A (n x n,
-// ld n; read only).  Eigenvalues ascending in w, the first nvec eigenvectors
-// in Z (ld n).
+// ld n; read only).  The lowest nvec eigenvalues ascending in w (all n when
+// nvec is 0), their eigenvectors in Z (ld n).
 void heev(cudaStream_t st, int n, double2* A, double* w, double2* Z, int nvec, Scratch& ws,
           const GemmWorkspace& gws);
 
