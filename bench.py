@@ -257,9 +257,12 @@ def config3_section(device):
     for name, prec in (("fp64", FP64), ("mixed", MIXED)):
         d = PlanewaveDavidsonDiagonalizer(ap, prec)
         d.set_tolerance(1e-14)
-        d.set_maximum_iterations(it)
         if prec == MIXED:
             d.set_precision(MIXED, 1e-14, 1)
+        # one untimed iteration first: the solver's buffers are allocated once
+        d.set_maximum_iterations(1)
+        d.solve(psi.clone(), nb)
+        d.set_maximum_iterations(it)
         r = d.solve(psi.clone(), nb)
         phase_s = r.seconds - (r.fp64_seconds if prec == MIXED else 0.0)
         phase_it = r.iterations - (r.fp64_iterations if prec == MIXED else 0)
@@ -267,6 +270,23 @@ def config3_section(device):
     res["iteration_ratio"] = res["iteration_ms_fp64"] / res["iteration_ms_mixed"]
     ap.ctx.close()
     return res
+
+
+def warm_server(srv, jobs, prec):
+    """Solve one short request per distinct FFT grid before timing: worker
+    buffers are allocated and the plane-kernel tile is tuned once per grid and
+    precision for the life of the process, as in a running server."""
+    grids, ids = set(), []
+    for sy, k in jobs:
+        if tuple(sy.cell.grid) in grids:
+            continue
+        grids.add(tuple(sy.cell.grid))
+        ids.append(srv.submit(sy, k=k, tolerance=1e-9, max_iterations=2, precision=prec))
+    for _ in range(max(0, 8 - len(ids))):
+        sy, k = jobs[0]
+        ids.append(srv.submit(sy, k=k, tolerance=1e-9, max_iterations=2, precision=prec))
+    for i in ids:
+        srv.wait(i)
 
 
 def davidson_section(ap, sy1, psi64, args):
@@ -329,6 +349,7 @@ def davidson_section(ap, sy1, psi64, args):
     k2 = {}
     for name, prec in (("fp64", FP64), ("mixed", MIXED)):
         srv = BandSolveServer(workers=8)
+        warm_server(srv, [(sy2, k) for k in range(len(sy2.kpoints))], prec)
         t0 = time.perf_counter()
         ids = [srv.submit(sy2, k=k, tolerance=1e-9, max_iterations=200, precision=prec)
                for k in range(len(sy2.kpoints))]
@@ -356,6 +377,7 @@ def davidson_section(ap, sy1, psi64, args):
     cap = {}
     for name, prec in (("fp64", FP64), ("mixed", MIXED)):
         srv = BandSolveServer(workers=8, hbm_budget=64 << 30)
+        warm_server(srv, [(sy, 0) for sy in systems], prec)
         t0 = time.perf_counter()
         ids = [srv.submit(sy, tolerance=TOL4, max_iterations=MAXIT4, precision=prec) for sy in systems]
         got = [srv.wait(i) for i in ids]
@@ -372,6 +394,7 @@ def davidson_section(ap, sy1, psi64, args):
     s4 = {}
     for name, prec in (("fp64", FP64), ("mixed", MIXED)):
         srv = BandSolveServer(workers=8, hbm_budget=64 << 30)
+        warm_server(srv, [(sy, 0) for sy in systems], prec)
         o = run_poisson_stream(srv, systems, rate_hz=rate, tolerance=TOL4,
                                max_iterations=MAXIT4, precision=prec)
         srv.close()

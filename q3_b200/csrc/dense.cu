@@ -573,9 +573,10 @@ __global__ void apply_phase(int n, int nvec, const double2* phase, const double*
 // p_{k-1} (exact), which keeps both in range, so the dependent chain per step
 // is one FMA, a select and a multiply.  S independent recurrences interleave.
 __device__ __forceinline__ double pow2_inverse_exponent(double p) {
-    const long long bits = __double_as_longlong(p);
-    const long long e = (bits >> 52) & 0x7ff;
-    return __longlong_as_double((2046 - e) << 52);
+    // the exponent field sits in bits 20..30 of the high word: 32-bit integer
+    // work only
+    const int e = (__double2hiint(p) >> 20) & 0x7ff;
+    return __hiloint2double((2046 - e) << 20, 0);
 }
 
 template <int S>
