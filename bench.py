@@ -53,9 +53,12 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=32)
     ap.add_argument("--serving-rate", type=float, default=0.0,
                     help="arrivals per second (default: 80%% of the measured FP64 capacity)")
-    ap.add_argument("--probe", choices=["mixed", "fp64"], default=None,
+    ap.add_argument("--probe", choices=["mixed", "fp64", "hegv"], default=None,
                     help="profiling aid: apply H to the bench block three times in one precision "
-                         "(after the plane-kernel tuning) and exit; prints no bench line")
+                         "(after the plane-kernel tuning), or run the subspace eigensolver on "
+                         "random problems of the --hegv-orders (hegv), and exit; prints no bench line")
+    ap.add_argument("--hegv-orders", default="16,32,64,96,128,192,256,384,512",
+                    help="orders for --probe hegv, comma separated")
     return ap.parse_args()
 
 
@@ -344,25 +347,31 @@ def davidson_section(ap, sy1, psi64, args):
                                                             res["fp64"][0].eigenvalues))) / 2.0,
         "speedup": res["mixed"][1] / res["fp64"][1],
     }
-    # (3) config 2: the 32 k-points, all submitted at once to 8 workers
+    # (3) config 2: the 32 k-points, all submitted at once to 8 workers; the
+    # batch three times on the same warm server, median wall time (the host
+    # threads that drive the requests share the machine's cores)
     sy2 = synthetic.config(2)
     k2 = {}
     for name, prec in (("fp64", FP64), ("mixed", MIXED)):
         srv = BandSolveServer(workers=8)
         warm_server(srv, [(sy2, k) for k in range(len(sy2.kpoints))], prec)
-        t0 = time.perf_counter()
-        ids = [srv.submit(sy2, k=k, tolerance=1e-9, max_iterations=200, precision=prec)
-               for k in range(len(sy2.kpoints))]
-        got = [srv.wait(i) for i in ids]
-        wall = time.perf_counter() - t0
+        walls = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            ids = [srv.submit(sy2, k=k, tolerance=1e-9, max_iterations=200, precision=prec)
+                   for k in range(len(sy2.kpoints))]
+            got = [srv.wait(i) for i in ids]
+            walls.append(time.perf_counter() - t0)
         srv.close()
-        k2[name] = (got, wall)
+        k2[name] = (got, statistics.median(walls), walls)
     err = max(float(np.max(np.abs(a.eigenvalues - b.eigenvalues)))
               for a, b in zip(k2["fp64"][0], k2["mixed"][0]))
     out["config2_kpoints"] = {
         "kpoints": len(sy2.kpoints), "tolerance_ry": 1e-9, "workers": 8,
-        "fp64": {"kpoints_per_s": len(sy2.kpoints) / k2["fp64"][1], "wall_s": k2["fp64"][1]},
-        "mixed": {"kpoints_per_s": len(sy2.kpoints) / k2["mixed"][1], "wall_s": k2["mixed"][1]},
+        "fp64": {"kpoints_per_s": len(sy2.kpoints) / k2["fp64"][1], "wall_s": k2["fp64"][1],
+                 "runs_s": k2["fp64"][2]},
+        "mixed": {"kpoints_per_s": len(sy2.kpoints) / k2["mixed"][1], "wall_s": k2["mixed"][1],
+                  "runs_s": k2["mixed"][2]},
         "mixed_vs_fp64_max_eig_err_ha": err / 2.0,
         "speedup": k2["fp64"][1] / k2["mixed"][1],
     }
@@ -374,14 +383,18 @@ def davidson_section(ap, sy1, psi64, args):
     TOL4 = 1e-9
     MAXIT4 = 300
     systems = synthetic.serving_requests(args.serving_requests)
-    cap = {}
+    cap, cap_runs = {}, {}
     for name, prec in (("fp64", FP64), ("mixed", MIXED)):
         srv = BandSolveServer(workers=8, hbm_budget=64 << 30)
         warm_server(srv, [(sy, 0) for sy in systems], prec)
-        t0 = time.perf_counter()
-        ids = [srv.submit(sy, tolerance=TOL4, max_iterations=MAXIT4, precision=prec) for sy in systems]
-        got = [srv.wait(i) for i in ids]
-        cap[name] = len(systems) / (time.perf_counter() - t0)
+        rates = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            ids = [srv.submit(sy, tolerance=TOL4, max_iterations=MAXIT4, precision=prec) for sy in systems]
+            got = [srv.wait(i) for i in ids]
+            rates.append(len(systems) / (time.perf_counter() - t0))
+        cap[name] = statistics.median(rates)
+        cap_runs[name] = rates
         srv.close()
         if name == "fp64":
             res64 = got
@@ -401,7 +414,8 @@ def davidson_section(ap, sy1, psi64, args):
         o.pop("results")
         s4[name] = o
     out["config4_serving"] = {"requests": len(systems), "tolerance_ry": TOL4,
-                              "capacity_solves_per_s": cap, "capacity_speedup": cap["mixed"] / cap["fp64"],
+                              "capacity_solves_per_s": cap, "capacity_runs": cap_runs,
+                              "capacity_speedup": cap["mixed"] / cap["fp64"],
                               "mixed_vs_fp64_max_eig_err_ha": err4 / 2.0,
                               "unconverged_in_capacity_run": unconv4, "max_iterations": MAXIT4,
                               "rate_hz": rate, "rate_rule": "0.8 x FP64 capacity",
@@ -593,9 +607,49 @@ def run_q3b(args):
         pg.destroy_process_group()
 
 
+def run_hegv_probe(args):
+    """The subspace eigensolver (q3b_hegv) on seeded random Hermitian H and
+    positive definite S of each order: five calls per order, the median wall
+    time of the last three (device buffers, one synchronisation per call)."""
+    import torch
+    from q3_b200 import synthetic
+    from q3_b200.applicator import PlanewaveHamiltonianApplicator
+    sy = synthetic.config(0)
+    ap = PlanewaveHamiltonianApplicator()
+    ap.update_potential(sy.v_r, sy.cell.grid)
+    ap.prepare_system_kpoint(sy)
+    dev = torch.device("cuda", ap.ctx.device)
+    out = {}
+    for n in (int(v) for v in args.hegv_orders.split(",") if v):
+        rng = np.random.default_rng(n)
+        x = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        y = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        h = (x + x.conj().T) / 2
+        s = y @ y.conj().T / n + np.eye(n)
+        H = torch.from_numpy(np.ascontiguousarray(h.T)).to(dev)
+        S = torch.from_numpy(np.ascontiguousarray(s.T)).to(dev)
+        w = torch.empty(n, dtype=torch.float64, device=dev)
+        Z = torch.empty(n, n, dtype=torch.complex128, device=dev)
+        torch.cuda.synchronize(dev)
+        ts = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            with ap.ctx.ordered_with_torch():
+                rc = ap.lib.q3b_hegv(ap.h, n, H.data_ptr(), S.data_ptr(), n, w.data_ptr(), Z.data_ptr())
+            torch.cuda.synchronize(dev)
+            ts.append(time.perf_counter() - t0)
+            if rc != 0:
+                raise RuntimeError(f"q3b_hegv failed at order {n}")
+        out[n] = 1e3 * float(np.median(ts[2:]))
+    print(json.dumps({"probe": "hegv", "ms": out}), flush=True)
+
+
 def run_probe(args):
     """Three H|psi> applications of the bench block in one precision: a short,
     fixed launch sequence for ncu captures of the plane and GEMM kernels."""
+    if args.probe == "hegv":
+        run_hegv_probe(args)
+        return
     import torch
     from q3_b200 import synthetic
     from q3_b200._lib import FP64, MIXED
