@@ -42,6 +42,11 @@ CASES = [
     dict(grid=(16, 16, 16), a=8.0, ecut=10.0, natoms=3),
     dict(grid=(24, 20, 18), a=9.0, ecut=9.0, natoms=4),
     dict(grid=(15, 15, 15), a=7.5, ecut=9.0, natoms=2, k_frac=(0.25, 0.125, 0.375)),
+    # lines with a factor above 10 (75 = 15 x 5, 96 = 12 x 8, 16 x 16): the
+    # kernels built for radices up to 16
+    dict(grid=(75, 16, 18), a=7.0, ecut=8.0, natoms=2),
+    dict(grid=(20, 96, 15), a=7.0, ecut=8.0, natoms=3, k_frac=(0.5, 0.0, 0.25)),
+    dict(grid=(256, 12, 12), a=7.0, ecut=8.0, natoms=2),
 ]
 
 
@@ -55,6 +60,7 @@ def test_hpsi_fp64_small(cuda_device, case):
     ref = ohpsi.apply_h(psi, kp, sy.v_r, sy.cell.grid)
     got = _run(ap, psi)
     assert _rel(got, ref) < FP64_TOL
+    assert _rel(_run(ap, psi, MIXED), ref) < FP32_TOL
 
 
 def test_hpsi_config0_fp64_and_mixed(cuda_device):
