@@ -15,6 +15,7 @@ namespace q3b {
 namespace {
 
 constexpr int kStickThreads = 256;
+constexpr int kLoadBatch = 4;      // global loads a stick-kernel thread keeps in flight
 constexpr int kRowMaskWords = 16;  // one word per item of the first column pass (nb1 <= 16)
 
 // Shared-memory set-up of the plane kernels: rowb[i] = w1 * p2 of the i-th
@@ -75,8 +76,22 @@ sticks_backward(LocalPlan<R> p, const cplx_t<R>* __restrict__ psi, long ldpsi, c
     __syncthreads();
     const T* ps = psi + (long)band * ldpsi;
     const int e0 = p.stick_start[s0], e1 = p.stick_start[s0 + ns];
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        lines[(p.entry_stick[e] - s0) * p.p3 + p.entry_w3[e]] = ps[p.entry_g[e]];
+    // kLoadBatch gathers in flight per thread before any is stored
+    for (int eb = e0 + threadIdx.x; eb < e1; eb += kLoadBatch * blockDim.x) {
+        T v[kLoadBatch];
+        int at[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int e = eb + u * blockDim.x;
+            at[u] = -1;
+            if (e < e1) {
+                at[u] = (p.entry_stick[e] - s0) * p.p3 + p.entry_w3[e];
+                v[u] = ps[p.entry_g[e]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u)
+            if (at[u] >= 0) lines[at[u]] = v[u];
     }
     __syncthreads();
     fft::LineGeom g{p.n3, p.na3, p.nb3, ns, p.p3, 1, nullptr};
@@ -141,9 +156,19 @@ sticks_forward(LocalPlan<R> p, const cplx_t<R>* __restrict__ X, const cplx_t<R>*
     const int ns = min(p.sg, p.nsticks - s0);
     for (int i = threadIdx.x; i < p.n3; i += blockDim.x) tw[i] = p.tw3[i];
     const T* xb = X + (long)band * p.n3 * p.nsticks;
-    for (int idx = threadIdx.x; idx < ns * p.n3; idx += blockDim.x) {
-        const int s = idx % ns, i3 = idx / ns;
-        lines[s * p.p3 + i3] = xb[(long)i3 * p.nsticks + s0 + s];
+    const int total = ns * p.n3;
+    for (int ib = threadIdx.x; ib < total; ib += kLoadBatch * blockDim.x) {
+        T v[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int idx = ib + u * blockDim.x;
+            if (idx < total) v[u] = xb[(long)(idx / ns) * p.nsticks + s0 + idx % ns];
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int idx = ib + u * blockDim.x;
+            if (idx < total) lines[(idx % ns) * p.p3 + idx / ns] = v[u];
+        }
     }
     __syncthreads();
     fft::LineGeom g{p.n3, p.na3, p.nb3, ns, p.p3, 1, nullptr};
@@ -151,10 +176,29 @@ sticks_forward(LocalPlan<R> p, const cplx_t<R>* __restrict__ X, const cplx_t<R>*
     const T* ps = psi + (long)band * ldpsi;
     T* hs = hpsi + (long)band * ldh;
     const int e0 = p.stick_start[s0], e1 = p.stick_start[s0 + ns];
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        const int gi = p.entry_g[e];
-        const T v = lines[(p.entry_stick[e] - s0) * p.p3 + p.entry_w3[e]];
-        hs[gi] = p.ke[gi] * ps[gi] + v;
+    for (int eb = e0 + threadIdx.x; eb < e1; eb += kLoadBatch * blockDim.x) {
+        int gi[kLoadBatch];
+        R ke[kLoadBatch];
+        T x[kLoadBatch], v[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int e = eb + u * blockDim.x;
+            gi[u] = -1;
+            if (e < e1) {
+                gi[u] = p.entry_g[e];
+                v[u] = lines[(p.entry_stick[e] - s0) * p.p3 + p.entry_w3[e]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            if (gi[u] >= 0) {
+                ke[u] = p.ke[gi[u]];
+                x[u] = ps[gi[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u)
+            if (gi[u] >= 0) hs[gi[u]] = ke[u] * x[u] + v[u];
     }
 }
 
