@@ -90,8 +90,82 @@ template <> struct Split<12> { static constexpr int A = 4, B = 3; };
 template <> struct Split<15> { static constexpr int A = 5, B = 3; };
 template <> struct Split<16> { static constexpr int A = 4, B = 4; };
 
-// In-register DFT of size N.  tw/tws: the line's table and n/N, so that
-// w_N^m = tw[m * tws].
+// cos(2 pi m / N) and sin(2 pi m / N) for m < N, the internal twiddles of the
+// composite small DFTs (plain trigonometry, evaluated in extended precision and
+// rounded to double)
+template <int N> __host__ __device__ constexpr double unit_cos(int m);
+template <int N> __host__ __device__ constexpr double unit_sin(int m);
+template <> __host__ __device__ constexpr double unit_cos<6>(int m) {
+    constexpr double t[6] = {1.0, 0.5, -0.5, -1.0, -0.5, 0.5};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_sin<6>(int m) {
+    constexpr double t[6] = {0.0, 0.8660254037844386, 0.8660254037844386, 0.0, -0.8660254037844386, -0.8660254037844386};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_cos<8>(int m) {
+    constexpr double t[8] = {1.0, 0.7071067811865476, 0.0, -0.7071067811865476, -1.0, -0.7071067811865476, 0.0, 0.7071067811865476};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_sin<8>(int m) {
+    constexpr double t[8] = {0.0, 0.7071067811865476, 1.0, 0.7071067811865476, 0.0, -0.7071067811865476, -1.0, -0.7071067811865476};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_cos<9>(int m) {
+    constexpr double t[9] = {1.0, 0.766044443118978, 0.17364817766693036, -0.5, -0.9396926207859084, -0.9396926207859084, -0.5, 0.17364817766693036, 0.766044443118978};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_sin<9>(int m) {
+    constexpr double t[9] = {0.0, 0.6427876096865394, 0.984807753012208, 0.8660254037844386, 0.3420201433256687, -0.3420201433256687, -0.8660254037844386, -0.984807753012208, -0.6427876096865394};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_cos<10>(int m) {
+    constexpr double t[10] = {1.0, 0.8090169943749475, 0.30901699437494745, -0.30901699437494745, -0.8090169943749475, -1.0, -0.8090169943749475, -0.30901699437494745, 0.30901699437494745, 0.8090169943749475};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_sin<10>(int m) {
+    constexpr double t[10] = {0.0, 0.5877852522924731, 0.9510565162951535, 0.9510565162951535, 0.5877852522924731, 0.0, -0.5877852522924731, -0.9510565162951535, -0.9510565162951535, -0.5877852522924731};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_cos<12>(int m) {
+    constexpr double t[12] = {1.0, 0.8660254037844386, 0.5, 0.0, -0.5, -0.8660254037844386, -1.0, -0.8660254037844386, -0.5, 0.0, 0.5, 0.8660254037844386};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_sin<12>(int m) {
+    constexpr double t[12] = {0.0, 0.5, 0.8660254037844386, 1.0, 0.8660254037844386, 0.5, 0.0, -0.5, -0.8660254037844386, -1.0, -0.8660254037844386, -0.5};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_cos<15>(int m) {
+    constexpr double t[15] = {1.0, 0.9135454576426009, 0.6691306063588582, 0.30901699437494745, -0.10452846326765347, -0.5, -0.8090169943749475, -0.9781476007338057, -0.9781476007338057, -0.8090169943749475, -0.5, -0.10452846326765347, 0.30901699437494745, 0.6691306063588582, 0.9135454576426009};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_sin<15>(int m) {
+    constexpr double t[15] = {0.0, 0.4067366430758002, 0.7431448254773942, 0.9510565162951535, 0.9945218953682733, 0.8660254037844386, 0.5877852522924731, 0.20791169081775934, -0.20791169081775934, -0.5877852522924731, -0.8660254037844386, -0.9945218953682733, -0.9510565162951535, -0.7431448254773942, -0.4067366430758002};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_cos<16>(int m) {
+    constexpr double t[16] = {1.0, 0.9238795325112867, 0.7071067811865476, 0.3826834323650898, 0.0, -0.3826834323650898, -0.7071067811865476, -0.9238795325112867, -1.0, -0.9238795325112867, -0.7071067811865476, -0.3826834323650898, 0.0, 0.3826834323650898, 0.7071067811865476, 0.9238795325112867};
+    return t[m];
+}
+template <> __host__ __device__ constexpr double unit_sin<16>(int m) {
+    constexpr double t[16] = {0.0, 0.3826834323650898, 0.7071067811865476, 0.9238795325112867, 1.0, 0.9238795325112867, 0.7071067811865476, 0.3826834323650898, 0.0, -0.3826834323650898, -0.7071067811865476, -0.9238795325112867, -1.0, -0.9238795325112867, -0.7071067811865476, -0.3826834323650898};
+    return t[m];
+}
+
+// x times w_N^m = exp(-2 pi i DIR' m / N) (conjugate for DIR = +1), m a constant
+// after unrolling: quarter turns are sign swaps, the rest a complex product
+// with literal constants.
+template <int N, int DIR, typename T> __device__ __forceinline__ T rotate_const(T x, int m) {
+    using R = typename RealOf<T>::R;
+    if (m == 0) return x;
+    if (4 * m == N) return DIR > 0 ? mul_i(x) : mk(x.y, -x.x);
+    if (2 * m == N) return mk(-x.x, -x.y);
+    if (4 * m == 3 * N) return DIR > 0 ? mk(x.y, -x.x) : mul_i(x);
+    return cmul(x, mk(R(unit_cos<N>(m)), R(DIR * unit_sin<N>(m))));
+}
+
+// In-register DFT of size N.  The internal twiddles of a composite N are
+// literal constants; tw/tws (the line's table and n/N) are not read.
 template <int N, int DIR, typename T>
 __device__ __forceinline__ void dft(T* x, const T* tw, int tws) {
     if constexpr (N == 1) {
@@ -114,10 +188,7 @@ __device__ __forceinline__ void dft(T* x, const T* tw, int tws) {
             for (int n1 = 0; n1 < A; ++n1) t[n1] = x[n2 + B * n1];
             dft<A, DIR>(t, tw, tws * B);
 #pragma unroll
-            for (int k1 = 0; k1 < A; ++k1) {
-                const int m = (n2 * k1) % N;
-                y[n2 + B * k1] = (m == 0) ? t[k1] : cmul(t[k1], twiddle<DIR>(tw, m * tws));
-            }
+            for (int k1 = 0; k1 < A; ++k1) y[n2 + B * k1] = rotate_const<N, DIR>(t[k1], (n2 * k1) % N);
         }
 #pragma unroll
         for (int k1 = 0; k1 < A; ++k1) {
