@@ -337,6 +337,37 @@ int q3b_start_rotate(q3b_context* ctx, const q3b_cplx128* coefficients_host, int
 int q3b_starting_subspace(q3b_context* ctx, const q3b_cplx128* chi_host, int nchi, int nb,
                           q3b_cplx128* bands_dev, double* eigenvalues_host);
 
+/* ---------------------------------------------------------------- Gamma-only k-point
+ * The reference's Gamma-only basis stores each band on the half sphere of G
+ * (the origin at index 0, then one of each +G/-G pair; basis/planewave/init.hpp:60-67)
+ * and applies H two real bands per complex transform
+ * (hamiltonian_applicator/serial.hpp:283-418) with real projector overlaps
+ * 2 Re(beta^H psi) less the origin's term (serial.hpp:519-566).
+ *
+ * prepare_kpoint for such a k-point (k = 0):
+ *   g_to_grid_host        npw_half grid indices of +G (-1 outside the grid); entry 0 the origin
+ *   g_minus_to_grid_host  npw_half grid indices of -G (serial.hpp:889-900); entry 0 equal to
+ *                         g_to_grid_host[0]
+ *   ke_host, beta_host    on the half sphere (npw_half x nproj, column-major); the projectors
+ *                         of a Gamma-only k-point satisfy beta(-G) = conj(beta(G)), which the
+ *                         library uses to extend them to the full sphere
+ *   atom offsets and D blocks as for q3b_prepare_kpoint.
+ * The library keeps the full-sphere plan (2 npw_half - 1 plane waves); q3b_apply_h
+ * then takes full-sphere vectors in the order [half sphere, mirrors of entries 1..]. */
+int q3b_prepare_kpoint_gamma(q3b_context* ctx, int npw_half, const int32_t* g_to_grid_host,
+                             const int32_t* g_minus_to_grid_host, const double* ke_host,
+                             const q3b_cplx128* beta_host, int nproj, int natoms,
+                             const int32_t* atom_proj_offsets_host, const double* d_blocks_host);
+
+/* apply_batch on a Gamma-only k-point (serial.hpp:283-418 and :519-566):
+ * hpsi = H psi for nvec half-sphere vectors (device, npw_half x nvec,
+ * column-major), bands 2p and 2p+1 through one complex transform.  The origin
+ * is packed as (Re psi_a(0), Re psi_b(0)) and hpsi(0) is real, as in the
+ * reference; a last band without a partner goes alone (the reference's
+ * single-band path).  Asynchronous on the context's stream, like q3b_apply_h. */
+int q3b_apply_h_gamma(q3b_context* ctx, const q3b_cplx128* psi_dev, q3b_cplx128* hpsi_dev, int nvec,
+                      int precision);
+
 #ifdef __cplusplus
 }
 #endif

@@ -111,6 +111,8 @@ SIGNATURES = {
     "q3b_prepare_kpoint_build": (_i, [_vp, _i, _vp, _vp, _vp, C.c_double, _i, _vp, _vp, _i, _vp, _vp, _i,
                                       C.c_double, _vp, _vp]),
     "q3b_get_projectors": (_i, [_vp, _vp, C.POINTER(_i)]),
+    "q3b_prepare_kpoint_gamma": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp]),
+    "q3b_apply_h_gamma": (_i, [_vp, _vp, _vp, _i, _i]),
     "q3b_start_apply": (_i, [_vp, _vp, _i]),
     "q3b_start_project": (_i, [_vp, _vp, _vp]),
     "q3b_start_rotate": (_i, [_vp, _vp, _i, _vp]),

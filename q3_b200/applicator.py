@@ -160,6 +160,49 @@ class PlanewaveHamiltonianApplicator:
             raise ValueError("vectors must be complex128 (or complex64 for the FP32 entry)")
         check(self.h, rc)
 
+    # Gamma-only k-point (serial.hpp:283-418, :519-566): half-sphere vectors, two bands per transform
+    def prepare_kpoint_gamma(self, number_of_plane_waves: int, g_vector_to_grid: np.ndarray,
+                             minus_g_vector_to_grid: np.ndarray, kinetic_energy_squared: np.ndarray,
+                             projectors: Optional[np.ndarray] = None,
+                             atom_proj_offsets: Optional[np.ndarray] = None,
+                             d_blocks: Optional[np.ndarray] = None) -> None:
+        """Half sphere of G with the origin at index 0: +G and -G grid indices, |G|^2 (Ry) and the
+        npw_half x P projectors (beta(-G) = conj(beta(G)) extends them to the full sphere)."""
+        npw = int(number_of_plane_waves)
+        g2g = np.ascontiguousarray(g_vector_to_grid, dtype=np.int32)
+        g2m = np.ascontiguousarray(minus_g_vector_to_grid, dtype=np.int32)
+        ke = np.ascontiguousarray(kinetic_energy_squared, dtype=np.float64)
+        if g2g.size != npw or g2m.size != npw or ke.size != npw:
+            raise ValueError("plane-wave arrays do not match number_of_plane_waves")
+        if projectors is None or projectors.shape[1] == 0:
+            rc = self.lib.q3b_prepare_kpoint_gamma(self.h, npw, _ptr(g2g), _ptr(g2m), _ptr(ke), None, 0, 0,
+                                                   None, None)
+        else:
+            beta = np.asfortranarray(projectors, dtype=np.complex128)
+            offs = np.ascontiguousarray(atom_proj_offsets, dtype=np.int32)
+            dblk = np.ascontiguousarray(d_blocks, dtype=np.float64)
+            if beta.shape[0] != npw:
+                raise ValueError("projector rows do not match number_of_plane_waves")
+            rc = self.lib.q3b_prepare_kpoint_gamma(self.h, npw, _ptr(g2g), _ptr(g2m), _ptr(ke), _ptr(beta),
+                                                   beta.shape[1], offs.size - 1, _ptr(offs), _ptr(dblk))
+        check(self.h, rc)
+        self.npw = 2 * npw - 1
+        self.gamma_npw = npw
+
+    def apply_batch_gamma(self, input_wavefunctions, output_hamiltonian_wavefunctions,
+                          number_of_vectors: int, precision: int = FP64) -> None:
+        """H on half-sphere vectors: complex128 device tensors laid out nvec x npw_half."""
+        psi, hpsi = input_wavefunctions, output_hamiltonian_wavefunctions
+        import torch
+        if psi.device.type != "cuda" or hpsi.device.type != "cuda":
+            raise ValueError("apply_batch_gamma takes device tensors")
+        if psi.dtype != torch.complex128 or hpsi.dtype != torch.complex128:
+            raise ValueError("vectors must be complex128")
+        with self.ctx.ordered_with_torch():
+            rc = self.lib.q3b_apply_h_gamma(self.h, psi.data_ptr(), hpsi.data_ptr(), int(number_of_vectors),
+                                            int(precision))
+        check(self.h, rc)
+
     def prepare_kpoint_build(self, kpoint_index: int, number_of_plane_waves: int, g_vector_to_grid: np.ndarray,
                              kinetic_energy_squared: np.ndarray, k_plus_g: np.ndarray, cell_volume: float,
                              positions: np.ndarray, species_of_atom: np.ndarray, beta_l, beta_tables: np.ndarray,

@@ -356,6 +356,7 @@ void Context::prepare_kpoint(int npw, const int32_t* g2g, const double* ke, cons
     if (nproj < 0 || (nproj > 0 && (!beta || natoms <= 0 || !offs || !dblk)))
         throw Status(Q3B_ERR_INVALID, "bad projector set");
     kp.valid = false;
+    gamma_half = 0;
     kp.npw = npw;
     kp.nproj = nproj;
     kp.natoms = natoms;

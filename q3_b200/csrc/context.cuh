@@ -84,6 +84,10 @@ class Context {
     DevBuf ws_start;
     int start_n = 0;
     int start_npw = 0;
+    // Gamma-only k-point: the half sphere's length (0 when the k-point was
+    // prepared with the full sphere) and the packed band pairs of q3b_apply_h_gamma
+    int gamma_half = 0;
+    DevBuf ws_gamma;
 
     // copy streams and events of q3b_apply_h_host's pipelined chunks
     static constexpr int kIoChunks = 4;

@@ -377,6 +377,36 @@ def serving_requests(count: int, seed: int = 1238) -> List[System]:
     return out
 
 
+@dataclasses.dataclass
+class GammaKPoint:
+    """A k = 0 point on the half sphere (the reference's Gamma-only basis): the origin first,
+    then every G whose first nonzero Miller index is positive."""
+    index: np.ndarray              # npw_half positions in the full-sphere list
+    g_to_grid: np.ndarray          # grid index of +G
+    minus_g_to_grid: np.ndarray    # grid index of -G (-1 outside the grid)
+    ke: np.ndarray
+    beta: np.ndarray               # npw_half x P
+    d_blocks: np.ndarray
+    atom_proj_offsets: np.ndarray
+
+    @property
+    def npw(self) -> int:
+        return int(self.index.size)
+
+
+def gamma_kpoint(system: "System", k: int = 0) -> GammaKPoint:
+    kp = system.kpoints[k]
+    if np.any(np.asarray(kp.k_frac) != 0.0):
+        raise ValueError("a Gamma-only basis needs k = 0")
+    m = kp.miller
+    first = np.where(m[:, 0] != 0, m[:, 0], np.where(m[:, 1] != 0, m[:, 1], m[:, 2]))
+    origin = np.flatnonzero(np.all(m == 0, axis=1))
+    index = np.concatenate([origin, np.flatnonzero(first > 0)]).astype(np.int64)
+    minus = grid_map(-m[index], system.cell.grid)
+    return GammaKPoint(index, kp.g_to_grid[index].astype(np.int32), minus.astype(np.int32), kp.ke[index],
+                       np.asfortranarray(kp.beta[index]), kp.d_blocks, kp.atom_proj_offsets)
+
+
 def small_system(grid=(12, 12, 12), a: float = 7.0, natoms: int = 2, ecut: float = 8.0,
                  nbands: int = 6, seed: int = 99, k_frac=(0.0, 0.0, 0.0),
                  lattice: Optional[np.ndarray] = None) -> System:

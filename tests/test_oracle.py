@@ -258,3 +258,29 @@ def test_projector_oracle_pieces_match_reference_kats():
             gram += w * (2 * np.pi / len(phis)) * np.outer(y, y)
     assert np.max(np.abs(gram - np.eye(len(gram)))) < 1e-12
     assert op.angular_phase(1) == -1j and op.angular_phase(6) == -1.0
+
+
+def test_gamma_oracle_is_the_full_sphere_operator():
+    """The Gamma restatement (two bands per transform, real overlaps) on states that are real in
+    real space gives the full-sphere oracle's H|psi> on the half sphere, for an even and an odd
+    band count."""
+    from oracle import gamma as og
+    sy = synthetic.small_system(nbands=5, grid=(16, 16, 16), a=8.0, ecut=10.0, natoms=3)
+    kp = sy.kpoints[0]
+    g = synthetic.gamma_kpoint(sy)
+    assert np.array_equal(g.index, og.half_sphere(kp.miller))
+    assert np.array_equal(g.minus_g_to_grid, og.minus_grid_index(kp.miller[g.index], sy.cell.grid))
+    key = {tuple(m): i for i, m in enumerate(kp.miller)}
+    mirror = np.array([key[tuple(-kp.miller[i])] for i in g.index])
+    assert 2 * g.npw - 1 == kp.npw
+    for nb in (4, 5):
+        rng = np.random.default_rng(nb)
+        ph = rng.standard_normal((g.npw, nb)) + 1j * rng.standard_normal((g.npw, nb))
+        ph[0] = ph[0].real
+        full = np.zeros((kp.npw, nb), complex)
+        full[g.index] = ph
+        full[mirror[1:]] = np.conj(ph[1:])
+        ref = hpsi.apply_h(full, kp, sy.v_r, sy.cell.grid)[g.index]
+        got = og.apply_h_gamma(ph, g.ke, g.g_to_grid, g.minus_g_to_grid, g.beta, g.d_blocks,
+                               g.atom_proj_offsets, sy.v_r, sy.cell.grid)
+        assert np.max(np.abs(got - ref)) < 1e-13 * np.max(np.abs(ref))
