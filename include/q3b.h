@@ -368,6 +368,28 @@ int q3b_prepare_kpoint_gamma(q3b_context* ctx, int npw_half, const int32_t* g_to
 int q3b_apply_h_gamma(q3b_context* ctx, const q3b_cplx128* psi_dev, q3b_cplx128* hpsi_dev, int nvec,
                       int precision);
 
+/* ---------------------------------------------------------------- ultrasoft overlap S
+ * UltrasoftPseudopotentialOverlapOperator (diagonalizer/planewave/internal/overlap/
+ * pseudopotential/ultrasoft/init.hpp:27-470): S psi = psi + sum_ij beta_i q_ij <beta_j|psi>.
+ *
+ * set the per-atom blocks q_ij of the prepared k-point (Ry-free, dimensionless), packed as
+ * the D blocks of q3b_prepare_kpoint (one m x m column-major block per atom; the reference's
+ * build_q_matrix, init.hpp:416-466, sets q_ab for equal l and m; entries |q| <= 1e-15 dropped).
+ * Preparing a k-point clears them. */
+int q3b_set_overlap_blocks(q3b_context* ctx, const double* q_blocks_host);
+
+/* apply_batch (init.hpp:189-345): spsi = S psi for nvec device vectors (npw x nvec,
+ * FP64 in and out; may be the same array).  Q3B_MIXED forms the correction
+ * beta Q beta^H psi with the FP32 tensor-core products and adds it to psi in FP64.
+ * Asynchronous on the context's stream. */
+int q3b_apply_s(q3b_context* ctx, const q3b_cplx128* psi_dev, q3b_cplx128* spsi_dev, int nvec,
+                int precision);
+
+/* The same on a Gamma-only k-point (init.hpp:212-270): half-sphere vectors, two bands
+ * per pass, separated as in q3b_apply_h_gamma. */
+int q3b_apply_s_gamma(q3b_context* ctx, const q3b_cplx128* psi_dev, q3b_cplx128* spsi_dev, int nvec,
+                      int precision);
+
 #ifdef __cplusplus
 }
 #endif

@@ -113,6 +113,9 @@ SIGNATURES = {
     "q3b_get_projectors": (_i, [_vp, _vp, C.POINTER(_i)]),
     "q3b_prepare_kpoint_gamma": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp]),
     "q3b_apply_h_gamma": (_i, [_vp, _vp, _vp, _i, _i]),
+    "q3b_set_overlap_blocks": (_i, [_vp, _vp]),
+    "q3b_apply_s": (_i, [_vp, _vp, _vp, _i, _i]),
+    "q3b_apply_s_gamma": (_i, [_vp, _vp, _vp, _i, _i]),
     "q3b_start_apply": (_i, [_vp, _vp, _i]),
     "q3b_start_project": (_i, [_vp, _vp, _vp]),
     "q3b_start_rotate": (_i, [_vp, _vp, _i, _vp]),

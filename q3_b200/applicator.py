@@ -203,6 +203,26 @@ class PlanewaveHamiltonianApplicator:
                                             int(precision))
         check(self.h, rc)
 
+    # UltrasoftPseudopotentialOverlapOperator (overlap/pseudopotential/ultrasoft/init.hpp)
+    def set_overlap_blocks(self, q_blocks: np.ndarray) -> None:
+        """Per-atom q_ij blocks, packed like the D blocks of the prepared k-point."""
+        q = np.ascontiguousarray(q_blocks, dtype=np.float64)
+        check(self.h, self.lib.q3b_set_overlap_blocks(self.h, _ptr(q)))
+
+    def apply_overlap(self, input_wavefunctions, output_wavefunctions, number_of_vectors: int,
+                      precision: int = FP64, gamma: bool = False) -> None:
+        """S psi on complex128 device tensors (nvec x npw; half-sphere vectors with gamma=True)."""
+        psi, spsi = input_wavefunctions, output_wavefunctions
+        import torch
+        if psi.device.type != "cuda" or spsi.device.type != "cuda":
+            raise ValueError("apply_overlap takes device tensors")
+        if psi.dtype != torch.complex128 or spsi.dtype != torch.complex128:
+            raise ValueError("vectors must be complex128")
+        fn = self.lib.q3b_apply_s_gamma if gamma else self.lib.q3b_apply_s
+        with self.ctx.ordered_with_torch():
+            rc = fn(self.h, psi.data_ptr(), spsi.data_ptr(), int(number_of_vectors), int(precision))
+        check(self.h, rc)
+
     def prepare_kpoint_build(self, kpoint_index: int, number_of_plane_waves: int, g_vector_to_grid: np.ndarray,
                              kinetic_energy_squared: np.ndarray, k_plus_g: np.ndarray, cell_volume: float,
                              positions: np.ndarray, species_of_atom: np.ndarray, beta_l, beta_tables: np.ndarray,

@@ -357,6 +357,8 @@ void Context::prepare_kpoint(int npw, const int32_t* g2g, const double* ke, cons
         throw Status(Q3B_ERR_INVALID, "bad projector set");
     kp.valid = false;
     gamma_half = 0;
+    kp.has_q = false;
+    kp.dpk_len = 0;
     kp.npw = npw;
     kp.nproj = nproj;
     kp.natoms = natoms;
@@ -406,6 +408,7 @@ void Context::prepare_kpoint(int npw, const int32_t* g2g, const double* ke, cons
         upload(this, kp.poff, po.data(), po.size());
         upload(this, kp.dpk64, d64.data(), d64.size());
         upload(this, kp.dpk32, d32.data(), d32.size());
+        kp.dpk_len = d64.size();
     }
     build_plan();
     kp.valid = true;
@@ -426,6 +429,31 @@ template <> NonlocalData<float> Context::nonlocal<float>() const {
         d.beta_accum = tc::PackedA{kp.beta_pk_accum.as<unsigned char>(), kp.npw, kp.nproj};
     }
     return d;
+}
+
+template <> NonlocalData<double> Context::overlap<double>() const {
+    NonlocalData<double> d = nonlocal<double>();
+    d.dpk = kp.qpk64.as<double>();
+    return d;
+}
+template <> NonlocalData<float> Context::overlap<float>() const {
+    NonlocalData<float> d = nonlocal<float>();
+    d.dpk = kp.qpk32.as<float>();
+    return d;
+}
+
+// Q blocks packed as the D blocks (per atom, column-major), the same 1e-15
+// threshold (ultrasoft/init.hpp:416-466 builds Q with d_matrix_element_threshold)
+void Context::set_overlap_blocks(const double* qblk) {
+    require_ready();
+    if (kp.nproj <= 0) throw Status(Q3B_ERR_STATE, "the k-point has no projectors");
+    if (!qblk) throw Status(Q3B_ERR_INVALID, "null overlap blocks");
+    std::vector<double> q64(kp.dpk_len);
+    for (size_t i = 0; i < kp.dpk_len; ++i) q64[i] = std::fabs(qblk[i]) > 1e-15 ? qblk[i] : 0.0;
+    std::vector<float> q32(q64.begin(), q64.end());
+    upload(this, kp.qpk64, q64.data(), q64.size());
+    upload(this, kp.qpk32, q32.data(), q32.size());
+    kp.has_q = true;
 }
 
 template <typename R> int Context::sticks_chunk(int nvec) const {

@@ -49,6 +49,9 @@ struct KPoint {
     DevBuf beta64, beta32;
     DevBuf beta_pk_overlap, beta_pk_accum;  // beta32 as packed tensor-core A tiles
     DevBuf pstart, psize, poff, dpk64, dpk32;
+    size_t dpk_len = 0;             // packed block entries (D, and Q when set)
+    bool has_q = false;             // ultrasoft overlap blocks set for this k-point
+    DevBuf qpk64, qpk32;
     // sticks plan
     DevBuf stick_start, entry_g, entry_w3, entry_stick, stick_pos, row_base, unmapped;
     DevBuf tw64[3], tw32[3];
@@ -105,6 +108,9 @@ class Context {
 
     template <typename R> const LocalPlan<R>& local_plan() const;
     template <typename R> NonlocalData<R> nonlocal() const;
+    // the same projectors with the ultrasoft overlap blocks Q in place of D
+    template <typename R> NonlocalData<R> overlap() const;
+    void set_overlap_blocks(const double* qblk);
     template <typename R> int sticks_chunk(int nvec) const;
 
     // H|psi> on device vectors in precision R (the solver's building block)
@@ -128,6 +134,12 @@ int fail(q3b_context* c, const std::exception& e);
 // kernel launches issued by the library so far
 unsigned long long launches();
 
+}  // namespace q3b
+
+namespace q3b {
+// S psi = psi + beta Q beta^H psi on device vectors of the prepared plan
+// (npw x nvec, FP64 in and out; MIXED computes the correction in FP32)
+void apply_s_device(Context& c, const double2* psi, double2* spsi, int nvec, int precision);
 }  // namespace q3b
 
 struct q3b_context {

@@ -177,3 +177,30 @@ int q3b_apply_h_gamma(q3b_context* ctx, const q3b_cplx128* psi, q3b_cplx128* hps
         Q3B_LAUNCH_CHECK();
     });
 }
+
+// The ultrasoft overlap operator on a Gamma-only k-point (ultrasoft/init.hpp:
+// 212-270 forms the real overlaps 2 Re(beta^H psi) less the origin's term):
+// the band pairs through S psi = psi + beta Q beta^H psi of the full-sphere
+// plan, separated as for H.
+int q3b_apply_s_gamma(q3b_context* ctx, const q3b_cplx128* psi, q3b_cplx128* spsi, int nvec, int precision) {
+    return gamma_guarded(ctx, [&](Context& c) {
+        c.require_ready();
+        if (c.gamma_half <= 0) throw q3b::Status(Q3B_ERR_STATE, "the k-point was not prepared as Gamma-only");
+        if (nvec < 0 || (nvec > 0 && (!psi || !spsi))) throw q3b::Status(Q3B_ERR_INVALID, "bad vectors");
+        if (nvec == 0) return;
+        const int nhalf = c.gamma_half, nfull = c.kp.npw;
+        const int npair = (nvec + 1) / 2;
+        const size_t n = (size_t)nfull * npair;
+        c.ws_gamma.reserve(&c, 2 * n * sizeof(double2));
+        double2* phi = c.ws_gamma.as<double2>();
+        double2* sphi = phi + n;
+        const long work = (long)nhalf * npair;
+        q3b::gamma_pack<<<q3b::grid_blocks(work), 256, 0, c.stream>>>(
+            nhalf, nvec, reinterpret_cast<const double2*>(psi), nhalf, phi, nfull);
+        Q3B_LAUNCH_CHECK();
+        q3b::apply_s_device(c, phi, sphi, npair, precision);
+        q3b::gamma_unpack<<<q3b::grid_blocks(work), 256, 0, c.stream>>>(
+            nhalf, nvec, sphi, nfull, reinterpret_cast<double2*>(spsi), nhalf);
+        Q3B_LAUNCH_CHECK();
+    });
+}

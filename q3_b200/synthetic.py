@@ -407,6 +407,23 @@ def gamma_kpoint(system: "System", k: int = 0) -> GammaKPoint:
                        np.asfortranarray(kp.beta[index]), kp.d_blocks, kp.atom_proj_offsets)
 
 
+def overlap_blocks(system: "System", seed: int = 4242, scale: float = 0.3) -> np.ndarray:
+    """Ultrasoft-style q_ij blocks for the system's projector layout, packed like its D blocks:
+    per atom, q couples projectors of the same l and m (the two s channels, and each m of the
+    two p channels), with a seeded symmetric 2 x 2 matrix per l."""
+    rng = np.random.default_rng(seed)
+    def sym():
+        a = rng.uniform(-scale, scale, size=(2, 2))
+        return 0.5 * (a + a.T)
+    qs, qp = sym(), sym()
+    blk = np.zeros((PROJECTORS_PER_ATOM, PROJECTORS_PER_ATOM))
+    blk[np.ix_([0, 1], [0, 1])] = qs
+    for m in range(3):
+        idx = [2 + m, 5 + m]
+        blk[np.ix_(idx, idx)] = qp
+    return np.concatenate([blk.reshape(-1, order="F")] * system.cell.natoms)
+
+
 def small_system(grid=(12, 12, 12), a: float = 7.0, natoms: int = 2, ecut: float = 8.0,
                  nbands: int = 6, seed: int = 99, k_frac=(0.0, 0.0, 0.0),
                  lattice: Optional[np.ndarray] = None) -> System:

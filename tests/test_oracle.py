@@ -284,3 +284,24 @@ def test_gamma_oracle_is_the_full_sphere_operator():
         got = og.apply_h_gamma(ph, g.ke, g.g_to_grid, g.minus_g_to_grid, g.beta, g.d_blocks,
                                g.atom_proj_offsets, sy.v_r, sy.cell.grid)
         assert np.max(np.abs(got - ref)) < 1e-13 * np.max(np.abs(ref))
+
+
+def test_gamma_overlap_oracle_is_the_full_sphere_operator():
+    """The Gamma restatement of S (real overlaps) equals the full-sphere S on states that are
+    real in real space, restricted to the half sphere."""
+    from oracle import overlap as oov
+    sy = synthetic.small_system(nbands=4, grid=(16, 16, 16), a=8.0, ecut=10.0, natoms=3)
+    kp = sy.kpoints[0]
+    g = synthetic.gamma_kpoint(sy)
+    q = synthetic.overlap_blocks(sy)
+    key = {tuple(m): i for i, m in enumerate(kp.miller)}
+    mirror = np.array([key[tuple(-kp.miller[i])] for i in g.index])
+    rng = np.random.default_rng(9)
+    ph = rng.standard_normal((g.npw, 4)) + 1j * rng.standard_normal((g.npw, 4))
+    ph[0] = ph[0].real
+    full = np.zeros((kp.npw, 4), complex)
+    full[g.index] = ph
+    full[mirror[1:]] = np.conj(ph[1:])
+    ref = oov.apply_s(full, kp.beta, q, kp.atom_proj_offsets)[g.index]
+    got = oov.apply_s_gamma(ph, g.beta, q, g.atom_proj_offsets)
+    assert np.max(np.abs(got - ref)) < 1e-13 * np.max(np.abs(ref))
