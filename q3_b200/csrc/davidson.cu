@@ -192,9 +192,10 @@ template <typename R> class Davidson {
     Davidson(Context& c, int nb, int expansion, DevBuf& mem, DevBuf& dmem)
         : c_(c), st_(c.stream), npw_(c.kp.npw), nb_(nb) {
         maxn_ = std::max(std::min(expansion * nb, npw_), nb);  // davidson.hpp:401-404
+        us_ = c.kp.has_q;
         const size_t vecs = (size_t)npw_ * maxn_;
         const size_t mm = (size_t)maxn_ * maxn_;
-        size_t bytes = 2 * vecs * sizeof(T) + (size_t)npw_ * maxn_ * sizeof(T)  // V, HV, tmp
+        size_t bytes = (us_ ? 3 : 2) * vecs * sizeof(T) + (size_t)npw_ * maxn_ * sizeof(T)  // V, HV, [SV], tmp
                        + 2 * mm * sizeof(double2)                                 // Hs, Ss
                        + 3 * mm * sizeof(double2)                                 // evec, gram64, uinv64
                        + 5 * mm * sizeof(T)                                       // evecR, cpack, cneg, coef, uinvR
@@ -204,6 +205,9 @@ template <typename R> class Davidson {
         Carve cv{mem.as<char>()};
         V_ = cv.take<T>(vecs);
         HV_ = cv.take<T>(vecs);
+        // S|V> has a buffer of its own only when S is not the identity
+        // (subspace_manager/serial.hpp:54-60 aliases it otherwise)
+        SV_ = us_ ? cv.take<T>(vecs) : V_;
         tmp_ = cv.take<T>((size_t)npw_ * maxn_);
         Hs_ = cv.take<double2>(mm);
         Ss_ = cv.take<double2>(mm);
@@ -245,12 +249,16 @@ template <typename R> class Davidson {
     int orthogonalize(int start, int ncand) {
         if (ncand == 0) return 0;
         T* Tc = V_ + (size_t)start * npw_;
+        T* STc = SV_ + (size_t)start * npw_;
+        apply_overlap(start, ncand);                                    // serial.hpp:62-68
         if (start > 0) {
-            gemm(true, start, ncand, npw_, one(), V_, npw_, Tc, npw_, zero(), coef_, start);
+            // C = V^H (S T); T -= V C, and S T -= (S V) C when S|V> is its own buffer
+            gemm(true, start, ncand, npw_, one(), V_, npw_, STc, npw_, zero(), coef_, start);
             gemm(false, npw_, ncand, start, mone(), V_, npw_, coef_, start, one(), Tc, npw_);
+            if (us_) gemm(false, npw_, ncand, start, mone(), SV_, npw_, coef_, start, one(), STc, npw_);
         }
-        // Cholesky QR, the Gram matrix and its factor in FP64
-        gemm(true, ncand, ncand, npw_, one(), Tc, npw_, Tc, npw_, zero(), coef_, ncand);
+        // Cholesky QR, the Gram matrix T^H S T and its factor in FP64
+        gemm(true, ncand, ncand, npw_, one(), Tc, npw_, STc, npw_, zero(), coef_, ncand);
         widen(ncand, ncand, coef_, ncand, gram_, ncand);
         dscratch_.used = 0;
         const int info = dense::potrf(st_, ncand, gram_, ncand, dscratch_);
@@ -261,8 +269,14 @@ template <typename R> class Davidson {
             const T* U = narrowed(ncand, ncand, uinv_, ncand, uinvR_);
             gemm(false, npw_, ncand, ncand, one(), Tc, npw_, U, ncand, zero(), tmp_, npw_);
             Q3B_CUDA(cudaMemcpyAsync(Tc, tmp_, (size_t)npw_ * ncand * sizeof(T), cudaMemcpyDeviceToDevice, st_));
+            if (us_) {
+                gemm(false, npw_, ncand, ncand, one(), STc, npw_, U, ncand, zero(), tmp_, npw_);
+                Q3B_CUDA(cudaMemcpyAsync(STc, tmp_, (size_t)npw_ * ncand * sizeof(T), cudaMemcpyDeviceToDevice,
+                                         st_));
+            }
             return ncand;
         }
+        if (us_) return mgs_overlap(start, ncand);
         // modified Gram-Schmidt fallback (serial.hpp:370-552)
         int accepted = 0;
         for (int cidx = 0; cidx < ncand; ++cidx) {
@@ -295,7 +309,7 @@ template <typename R> class Davidson {
     void update(int start, int nnew, int total) {
         if (nnew <= 0) return;
         const T* Hn = HV_ + (size_t)start * npw_;
-        const T* Sn = V_ + (size_t)start * npw_;
+        const T* Sn = SV_ + (size_t)start * npw_;
         if constexpr (std::is_same<R, double>::value) {
             gemm(true, total, nnew, npw_, one(), V_, npw_, Hn, npw_, zero(), Hs_ + (size_t)start * maxn_, maxn_);
             gemm(true, total, nnew, npw_, one(), V_, npw_, Sn, npw_, zero(), Ss_ + (size_t)start * maxn_, maxn_);
@@ -333,7 +347,7 @@ template <typename R> class Davidson {
                                                                              cpack_, cneg_, eps_);
         Q3B_LAUNCH_CHECK();
         T* Rc = V_ + (size_t)basis * npw_;
-        gemm(false, npw_, ncand, basis, one(), V_, npw_, cneg_, basis, zero(), Rc, npw_);   // -(SV)c eps
+        gemm(false, npw_, ncand, basis, one(), SV_, npw_, cneg_, basis, zero(), Rc, npw_);  // -(SV)c eps
         gemm(false, npw_, ncand, basis, one(), HV_, npw_, cpack_, basis, one(), Rc, npw_);  // + (HV)c
         precondition_kernel<R><<<grid_for((long)npw_ * ncand), 256, 0, st_>>>(npw_, ncand, ke_, eps_, Rc);
         Q3B_LAUNCH_CHECK();
@@ -348,6 +362,10 @@ template <typename R> class Davidson {
         Q3B_CUDA(cudaMemcpyAsync(V_, tmp_, bytes, cudaMemcpyDeviceToDevice, st_));
         gemm(false, npw_, nb_, basis, one(), HV_, npw_, C, basis, zero(), tmp_, npw_);
         Q3B_CUDA(cudaMemcpyAsync(HV_, tmp_, bytes, cudaMemcpyDeviceToDevice, st_));
+        if (us_) {
+            gemm(false, npw_, nb_, basis, one(), SV_, npw_, C, basis, zero(), tmp_, npw_);
+            Q3B_CUDA(cudaMemcpyAsync(SV_, tmp_, bytes, cudaMemcpyDeviceToDevice, st_));
+        }
     }
 
     // --------------------------------------- collapse_subspace (serial.hpp:825-945)
@@ -359,7 +377,7 @@ template <typename R> class Davidson {
             T* h = coef_;
             gemm(true, basis, basis, npw_, one(), V_, npw_, HV_, npw_, zero(), h, basis);
             widen(basis, basis, h, basis, gram_, basis);
-            gemm(true, basis, basis, npw_, one(), V_, npw_, V_, npw_, zero(), h, basis);
+            gemm(true, basis, basis, npw_, one(), V_, npw_, SV_, npw_, zero(), h, basis);
             widen(basis, basis, h, basis, uinv_, basis);
             info = diagonalize(basis, gram_, uinv_, basis, false);
             if (info != 0) throw Status(Q3B_ERR_LINALG, "subspace eigensolver failed in the collapse");
@@ -389,7 +407,7 @@ template <typename R> class Davidson {
             pack_coefficients<R><<<grid_for((long)basis * nb_), 256, 0, st_>>>(basis, nb_, evec_, idx_, w_,
                                                                                cpack_, cneg_, eps_);
             Q3B_LAUNCH_CHECK();
-            gemm(false, npw_, nb_, basis, one(), V_, npw_, cneg_, basis, zero(), tmp_, npw_);
+            gemm(false, npw_, nb_, basis, one(), SV_, npw_, cneg_, basis, zero(), tmp_, npw_);
             gemm(false, npw_, nb_, basis, one(), HV_, npw_, cpack_, basis, one(), tmp_, npw_);
             column_norms<R><<<nb_, 256, 0, st_>>>(npw_, tmp_, norms_);
             Q3B_LAUNCH_CHECK();
@@ -398,6 +416,61 @@ template <typename R> class Davidson {
             Q3B_CUDA(cudaStreamSynchronize(st_));
             *resid_max = *std::max_element(h, h + nb_);
         }
+    }
+
+    // S|V> for columns [first, first+count): V + beta Q beta^H V (the
+    // ultrasoft operator, overlap/pseudopotential/ultrasoft/init.hpp:189-345)
+    void apply_overlap(int first, int count) {
+        if (!us_ || count <= 0) return;
+        T* v = V_ + (size_t)first * npw_;
+        T* sv = SV_ + (size_t)first * npw_;
+        Q3B_CUDA(cudaMemcpyAsync(sv, v, (size_t)npw_ * count * sizeof(T), cudaMemcpyDeviceToDevice, st_));
+        const int P = c_.kp.nproj;
+        const size_t pb = (size_t)P * count * sizeof(T);
+        c_.ws_bm.reserve(&c_, pb);
+        c_.ws_bp.reserve(&c_, pb);
+        GemmWorkspace ws = c_.gemm_ws(cgemm_workspace_bytes<R>(P, count, npw_));
+        apply_nonlocal<R>(st_, c_.overlap<R>(), npw_, count, v, npw_, sv, npw_, c_.ws_bm.as<T>(),
+                          c_.ws_bp.as<T>(), ws);
+    }
+
+    // modified Gram-Schmidt in the S metric (the Cholesky-QR fallback,
+    // serial.hpp:370-552, with S|v> carried beside every v)
+    int mgs_overlap(int start, int ncand) {
+        int accepted = 0;
+        for (int cidx = 0; cidx < ncand; ++cidx) {
+            const int src = start + cidx, dst = start + accepted;
+            T* v = V_ + (size_t)dst * npw_;
+            T* sv = SV_ + (size_t)dst * npw_;
+            if (dst != src) {
+                Q3B_CUDA(cudaMemcpyAsync(v, V_ + (size_t)src * npw_, npw_ * sizeof(T), cudaMemcpyDeviceToDevice, st_));
+                Q3B_CUDA(cudaMemcpyAsync(sv, SV_ + (size_t)src * npw_, npw_ * sizeof(T), cudaMemcpyDeviceToDevice,
+                                         st_));
+            }
+            const int nex = dst - start;
+            if (nex > 0) {
+                const T* B = V_ + (size_t)start * npw_;
+                const T* SB = SV_ + (size_t)start * npw_;
+                gemm(true, nex, 1, npw_, one(), B, npw_, sv, npw_, zero(), coef_, nex);
+                gemm(false, npw_, 1, nex, mone(), B, npw_, coef_, nex, one(), v, npw_);
+                gemm(false, npw_, 1, nex, mone(), SB, npw_, coef_, nex, one(), sv, npw_);
+            }
+            // ||v||_S^2 = Re v^H S v
+            gemm(true, 1, 1, npw_, one(), v, npw_, sv, npw_, zero(), coef_, 1);
+            T* hb = static_cast<T*>(host_readback(sizeof(T)));
+            Q3B_CUDA(cudaMemcpyAsync(hb, coef_, sizeof(T), cudaMemcpyDeviceToHost, st_));
+            Q3B_CUDA(cudaStreamSynchronize(st_));
+            const double n2 = static_cast<double>(hb[0].x);
+            if (n2 > kNormThreshold) {
+                const double inv = 1.0 / std::sqrt(n2);
+                scale_vector<R><<<grid_for(npw_), 256, 0, st_>>>(npw_, v, inv);
+                Q3B_LAUNCH_CHECK();
+                scale_vector<R><<<grid_for(npw_), 256, 0, st_>>>(npw_, sv, inv);
+                Q3B_LAUNCH_CHECK();
+                ++accepted;
+            }
+        }
+        return accepted;
     }
 
     void apply(int first, int count) {
@@ -571,7 +644,8 @@ template <typename R> class Davidson {
     cudaStream_t st_;
     int npw_, nb_, maxn_ = 0;
     int happly_ = 0;
-    T *V_, *HV_, *tmp_, *evecR_, *cpack_, *cneg_, *coef_, *uinvR_;
+    T *V_, *HV_, *SV_, *tmp_, *evecR_, *cpack_, *cneg_, *coef_, *uinvR_;
+    bool us_ = false;  // S is not the identity (ultrasoft overlap blocks set)
     double2 *Hs_, *Ss_, *evec_, *gram_, *uinv_;
     double *w_, *eps_, *norms_;
     int* idx_;

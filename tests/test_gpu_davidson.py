@@ -207,3 +207,36 @@ def test_hegv_graph_replay_is_bitwise_the_direct_solve(cuda_device, ctx_app, n):
         assert np.array_equal(wk, out[0][0]) and np.array_equal(zk, out[0][1])
     we = odav.diagonalize_subspace(h, s, n)[0]
     assert np.max(np.abs(out[4][0] - we)) < 1e-12 * max(1.0, np.max(np.abs(we))) * max(1, n / 16)
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+def test_davidson_ultrasoft_generalized(cuda_device, ctx_app, precision):
+    """With overlap blocks set the solve is the generalized problem H c = eps S c (the ultrasoft
+    overlap operator in the subspace manager's S|V> buffer): the eigenvalues match the dense
+    generalized problem and the bands come back S-orthonormal."""
+    import scipy.linalg as sl
+    from oracle import overlap as oov
+    from q3_b200.davidson import PlanewaveDavidsonDiagonalizer
+    sy = synthetic.small_system(nbands=6, grid=(12, 12, 12), a=7.0, ecut=8.0, natoms=2, seed=21)
+    kp = sy.kpoints[0]
+    q = synthetic.overlap_blocks(sy, scale=0.2)
+    _prep(ctx_app, sy)
+    ctx_app.set_overlap_blocks(q)
+    h = odense(kp, sy)
+    s = oov.apply_s(np.eye(kp.npw, dtype=complex), kp.beta, q, kp.atom_proj_offsets)
+    exact = sl.eigh(h, s, eigvals_only=True)[:sy.nbands]
+    dv = PlanewaveDavidsonDiagonalizer(ctx_app, precision)
+    dv.set_tolerance(1e-11)
+    dv.set_maximum_iterations(200)
+    if precision == MIXED:
+        dv.set_precision(MIXED, refine_sweeps=200)
+    r = dv.solve(sy.psi0[0], sy.nbands)
+    assert r.unconverged == 0
+    assert np.max(np.abs(r.eigenvalues - exact)) < 1e-8
+    z = r.bands
+    assert np.max(np.abs(z.conj().T @ s @ z - np.eye(sy.nbands))) < 1e-8
+    assert np.max(np.abs(h @ z - (s @ z) * r.eigenvalues[None, :])) < 1e-4
+
+
+def odense(kp, sy):
+    return ohpsi.dense_hamiltonian(kp, sy.v_r, sy.cell.grid)
