@@ -94,6 +94,7 @@ def apply_local_gamma(psi: np.ndarray, ke: np.ndarray, g2g: np.ndarray, g2g_minu
     return out
 
 
+
 def apply_nonlocal_gamma(psi: np.ndarray, beta: np.ndarray, d_blocks: np.ndarray,
                          atom_proj_offsets: np.ndarray) -> np.ndarray:
     """serial.hpp:519-566: real overlaps 2 Re(beta^H psi) - Re(conj beta(0) psi(0)), then D per

@@ -296,8 +296,8 @@ int q3b_davidson_solve(q3b_context* ctx, q3b_cplx128* bands, double* eig, int nb
     return guarded(ctx, [&](Context& c) {
         if (!bands || !eig || !opts) throw q3b::Status(Q3B_ERR_INVALID, "null argument");
         c.require_ready();
-        if (nb <= 0 || nb > c.kp.npw) throw q3b::Status(Q3B_ERR_INVALID, "band count must be in [1, npw]");
-        const size_t bytes = (size_t)c.kp.npw * nb * sizeof(double2);
+        if (nb <= 0 || nb > c.band_npw()) throw q3b::Status(Q3B_ERR_INVALID, "band count must be in [1, npw]");
+        const size_t bytes = (size_t)c.band_npw() * nb * sizeof(double2);
         c.ws_bands.reserve(&c, bytes);
         Q3B_CUDA(cudaMemcpyAsync(c.ws_bands.ptr, bands, bytes, cudaMemcpyHostToDevice, c.stream));
         q3b::davidson_solve(c, c.ws_bands.as<double2>(), eig, nb, *opts, stats);

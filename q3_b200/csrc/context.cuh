@@ -91,6 +91,8 @@ class Context {
     // prepared with the full sphere) and the packed band pairs of q3b_apply_h_gamma
     int gamma_half = 0;
     DevBuf ws_gamma;
+    // length of a band vector of the prepared k-point (the half sphere at Gamma)
+    int band_npw() const { return gamma_half > 0 ? gamma_half : kp.npw; }
 
     // copy streams and events of q3b_apply_h_host's pipelined chunks
     static constexpr int kIoChunks = 4;

@@ -25,6 +25,7 @@
 
 #include "davidson.cuh"
 #include "dense.cuh"
+#include "gamma.cuh"
 #include "nonlocal.cuh"
 
 namespace q3b {
@@ -126,9 +127,10 @@ __global__ void narrow_block(int M, int N, const double2* __restrict__ src, int 
     }
 }
 
-// out[j] = ||X[:, j]||, one block per column, fixed-order reduction
+// out[j] = ||X[:, j]||, one block per column, fixed-order reduction; with
+// gamma the half-sphere norm sqrt(2 sum |x|^2 - |x_0|^2)
 template <typename R>
-__global__ void column_norms(int npw, const cplx_t<R>* __restrict__ X, double* out) {
+__global__ void column_norms(int npw, const cplx_t<R>* __restrict__ X, double* out, int gamma = 0) {
     const cplx_t<R>* x = X + (long)blockIdx.x * npw;
     double s = 0.0;
     for (int g = threadIdx.x; g < npw; g += blockDim.x) {
@@ -142,7 +144,30 @@ __global__ void column_norms(int npw, const cplx_t<R>* __restrict__ X, double* o
         if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[blockIdx.x] = sqrt(red[0]);
+    if (threadIdx.x == 0) {
+        double t = red[0];
+        if (gamma) {
+            const cplx_t<R> v0 = x[0];
+            t = 2.0 * t - ((double)v0.x * v0.x + (double)v0.y * v0.y);
+        }
+        out[blockIdx.x] = sqrt(t > 0.0 ? t : 0.0);
+    }
+}
+
+// Gamma-only inner products of half-sphere vectors (the subspace manager's
+// gamma branches, e.g. subspace_manager/serial.hpp:72-110): C = 2 Re(A^H B)
+// less the origin's Re(conj(A_0) B_0), real
+template <typename T>
+__global__ void gamma_inner_fix(int M, int N, const T* __restrict__ A, long lda, const T* __restrict__ B, long ldb,
+                                T* C, long ldc) {
+    const long total = (long)M * N;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const int i = static_cast<int>(t % M), j = static_cast<int>(t / M);
+        const T c = C[i + (long)j * ldc];
+        const T a0 = A[(long)i * lda], b0 = B[(long)j * ldb];
+        const double re = 2.0 * (double)c.x - ((double)a0.x * b0.x + (double)a0.y * b0.y);
+        C[i + (long)j * ldc] = mk(static_cast<decltype(c.x)>(re), static_cast<decltype(c.x)>(0));
+    }
 }
 
 __global__ void set_identity(int n, double2* E) {
@@ -190,12 +215,16 @@ template <typename R> class Davidson {
     using T = cplx_t<R>;
 
     Davidson(Context& c, int nb, int expansion, DevBuf& mem, DevBuf& dmem)
-        : c_(c), st_(c.stream), npw_(c.kp.npw), nb_(nb) {
+        : c_(c), st_(c.stream), npw_(c.band_npw()), nb_(nb) {
         maxn_ = std::max(std::min(expansion * nb, npw_), nb);  // davidson.hpp:401-404
         us_ = c.kp.has_q;
+        gamma_ = c.gamma_half > 0;
         const size_t vecs = (size_t)npw_ * maxn_;
         const size_t mm = (size_t)maxn_ * maxn_;
+        // Gamma-only: band pairs packed into full-sphere vectors for H and S
+        const size_t gvecs = gamma_ ? (size_t)c.kp.npw * ((maxn_ + 1) / 2) : 0;
         size_t bytes = (us_ ? 3 : 2) * vecs * sizeof(T) + (size_t)npw_ * maxn_ * sizeof(T)  // V, HV, [SV], tmp
+                       + 2 * gvecs * sizeof(T)                                            // packed pairs
                        + 2 * mm * sizeof(double2)                                 // Hs, Ss
                        + 3 * mm * sizeof(double2)                                 // evec, gram64, uinv64
                        + 5 * mm * sizeof(T)                                       // evecR, cpack, cneg, coef, uinvR
@@ -208,6 +237,10 @@ template <typename R> class Davidson {
         // S|V> has a buffer of its own only when S is not the identity
         // (subspace_manager/serial.hpp:54-60 aliases it otherwise)
         SV_ = us_ ? cv.take<T>(vecs) : V_;
+        if (gamma_) {
+            gphi_ = cv.take<T>(gvecs);
+            ghphi_ = cv.take<T>(gvecs);
+        }
         tmp_ = cv.take<T>((size_t)npw_ * maxn_);
         Hs_ = cv.take<double2>(mm);
         Ss_ = cv.take<double2>(mm);
@@ -241,6 +274,15 @@ template <typename R> class Davidson {
         GemmWorkspace ws = c_.gemm_ws(conj ? cgemm_workspace_bytes<R>(M, N, K) : 0);
         cgemm<R>(st_, conj, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, ws);
     }
+    // inner products A^H B (K = npw): on a Gamma-only k-point the real
+    // half-sphere form
+    void inner(int M, int N, const T* A, const T* B, T* C, long ldc) {
+        gemm(true, M, N, npw_, one(), A, npw_, B, npw_, zero(), C, ldc);
+        if (gamma_) {
+            gamma_inner_fix<T><<<grid_for((long)M * N), 256, 0, st_>>>(M, N, A, npw_, B, npw_, C, ldc);
+            Q3B_LAUNCH_CHECK();
+        }
+    }
     static T one() { return mk(R(1), R(0)); }
     static T zero() { return mk(R(0), R(0)); }
     static T mone() { return mk(R(-1), R(0)); }
@@ -250,15 +292,19 @@ template <typename R> class Davidson {
         if (ncand == 0) return 0;
         T* Tc = V_ + (size_t)start * npw_;
         T* STc = SV_ + (size_t)start * npw_;
+        if (gamma_) {
+            gamma_real_origin<T><<<1, 256, 0, st_>>>(ncand, Tc, npw_);
+            Q3B_LAUNCH_CHECK();
+        }
         apply_overlap(start, ncand);                                    // serial.hpp:62-68
         if (start > 0) {
             // C = V^H (S T); T -= V C, and S T -= (S V) C when S|V> is its own buffer
-            gemm(true, start, ncand, npw_, one(), V_, npw_, STc, npw_, zero(), coef_, start);
+            inner(start, ncand, V_, STc, coef_, start);
             gemm(false, npw_, ncand, start, mone(), V_, npw_, coef_, start, one(), Tc, npw_);
             if (us_) gemm(false, npw_, ncand, start, mone(), SV_, npw_, coef_, start, one(), STc, npw_);
         }
         // Cholesky QR, the Gram matrix T^H S T and its factor in FP64
-        gemm(true, ncand, ncand, npw_, one(), Tc, npw_, STc, npw_, zero(), coef_, ncand);
+        inner(ncand, ncand, Tc, STc, coef_, ncand);
         widen(ncand, ncand, coef_, ncand, gram_, ncand);
         dscratch_.used = 0;
         const int info = dense::potrf(st_, ncand, gram_, ncand, dscratch_);
@@ -286,10 +332,10 @@ template <typename R> class Davidson {
                 Q3B_CUDA(cudaMemcpyAsync(v, V_ + (size_t)src * npw_, npw_ * sizeof(T), cudaMemcpyDeviceToDevice, st_));
             const int nex = dst - start;
             if (nex > 0) {
-                gemm(true, nex, 1, npw_, one(), Tc, npw_, v, npw_, zero(), coef_, nex);
+                inner(nex, 1, Tc, v, coef_, nex);
                 gemm(false, npw_, 1, nex, mone(), Tc, npw_, coef_, nex, one(), v, npw_);
             }
-            column_norms<R><<<1, 256, 0, st_>>>(npw_, v, norms_);
+            column_norms<R><<<1, 256, 0, st_>>>(npw_, v, norms_, gamma_ ? 1 : 0);
             Q3B_LAUNCH_CHECK();
             double* hb = static_cast<double*>(host_readback(sizeof(double)));
             Q3B_CUDA(cudaMemcpyAsync(hb, norms_, sizeof(double), cudaMemcpyDeviceToHost, st_));
@@ -311,12 +357,12 @@ template <typename R> class Davidson {
         const T* Hn = HV_ + (size_t)start * npw_;
         const T* Sn = SV_ + (size_t)start * npw_;
         if constexpr (std::is_same<R, double>::value) {
-            gemm(true, total, nnew, npw_, one(), V_, npw_, Hn, npw_, zero(), Hs_ + (size_t)start * maxn_, maxn_);
-            gemm(true, total, nnew, npw_, one(), V_, npw_, Sn, npw_, zero(), Ss_ + (size_t)start * maxn_, maxn_);
+            inner(total, nnew, V_, Hn, Hs_ + (size_t)start * maxn_, maxn_);
+            inner(total, nnew, V_, Sn, Ss_ + (size_t)start * maxn_, maxn_);
         } else {
-            gemm(true, total, nnew, npw_, one(), V_, npw_, Hn, npw_, zero(), coef_, total);
+            inner(total, nnew, V_, Hn, coef_, total);
             widen(total, nnew, coef_, total, Hs_ + (size_t)start * maxn_, maxn_);
-            gemm(true, total, nnew, npw_, one(), V_, npw_, Sn, npw_, zero(), coef_, total);
+            inner(total, nnew, V_, Sn, coef_, total);
             widen(total, nnew, coef_, total, Ss_ + (size_t)start * maxn_, maxn_);
         }
     }
@@ -375,9 +421,9 @@ template <typename R> class Davidson {
         if (info != 0) {
             // rebuild the subspace from the vectors
             T* h = coef_;
-            gemm(true, basis, basis, npw_, one(), V_, npw_, HV_, npw_, zero(), h, basis);
+            inner(basis, basis, V_, HV_, h, basis);
             widen(basis, basis, h, basis, gram_, basis);
-            gemm(true, basis, basis, npw_, one(), V_, npw_, SV_, npw_, zero(), h, basis);
+            inner(basis, basis, V_, SV_, h, basis);
             widen(basis, basis, h, basis, uinv_, basis);
             info = diagonalize(basis, gram_, uinv_, basis, false);
             if (info != 0) throw Status(Q3B_ERR_LINALG, "subspace eigensolver failed in the collapse");
@@ -409,7 +455,7 @@ template <typename R> class Davidson {
             Q3B_LAUNCH_CHECK();
             gemm(false, npw_, nb_, basis, one(), SV_, npw_, cneg_, basis, zero(), tmp_, npw_);
             gemm(false, npw_, nb_, basis, one(), HV_, npw_, cpack_, basis, one(), tmp_, npw_);
-            column_norms<R><<<nb_, 256, 0, st_>>>(npw_, tmp_, norms_);
+            column_norms<R><<<nb_, 256, 0, st_>>>(npw_, tmp_, norms_, gamma_ ? 1 : 0);
             Q3B_LAUNCH_CHECK();
             double* h = static_cast<double*>(host_readback(nb_ * sizeof(double)));
             Q3B_CUDA(cudaMemcpyAsync(h, norms_, nb_ * sizeof(double), cudaMemcpyDeviceToHost, st_));
@@ -422,16 +468,31 @@ template <typename R> class Davidson {
     // ultrasoft operator, overlap/pseudopotential/ultrasoft/init.hpp:189-345)
     void apply_overlap(int first, int count) {
         if (!us_ || count <= 0) return;
-        T* v = V_ + (size_t)first * npw_;
+        const T* v = V_ + (size_t)first * npw_;
         T* sv = SV_ + (size_t)first * npw_;
-        Q3B_CUDA(cudaMemcpyAsync(sv, v, (size_t)npw_ * count * sizeof(T), cudaMemcpyDeviceToDevice, st_));
+        const int nfull = c_.kp.npw;
+        // on a Gamma-only k-point the band pairs go through S on the full sphere
+        const int nv = gamma_ ? (count + 1) / 2 : count;
+        const T* in = v;
+        T* out = sv;
+        if (gamma_) {
+            gamma_pack<T><<<gamma_blocks((long)npw_ * nv), 256, 0, st_>>>(npw_, count, v, npw_, gphi_, nfull);
+            Q3B_LAUNCH_CHECK();
+            in = gphi_;
+            out = ghphi_;
+        }
+        const int len = gamma_ ? nfull : npw_;
+        Q3B_CUDA(cudaMemcpyAsync(out, in, (size_t)len * nv * sizeof(T), cudaMemcpyDeviceToDevice, st_));
         const int P = c_.kp.nproj;
-        const size_t pb = (size_t)P * count * sizeof(T);
+        const size_t pb = (size_t)P * nv * sizeof(T);
         c_.ws_bm.reserve(&c_, pb);
         c_.ws_bp.reserve(&c_, pb);
-        GemmWorkspace ws = c_.gemm_ws(cgemm_workspace_bytes<R>(P, count, npw_));
-        apply_nonlocal<R>(st_, c_.overlap<R>(), npw_, count, v, npw_, sv, npw_, c_.ws_bm.as<T>(),
-                          c_.ws_bp.as<T>(), ws);
+        GemmWorkspace ws = c_.gemm_ws(cgemm_workspace_bytes<R>(P, nv, len));
+        apply_nonlocal<R>(st_, c_.overlap<R>(), len, nv, in, len, out, len, c_.ws_bm.as<T>(), c_.ws_bp.as<T>(), ws);
+        if (gamma_) {
+            gamma_unpack<T><<<gamma_blocks((long)npw_ * nv), 256, 0, st_>>>(npw_, count, ghphi_, nfull, sv, npw_);
+            Q3B_LAUNCH_CHECK();
+        }
     }
 
     // modified Gram-Schmidt in the S metric (the Cholesky-QR fallback,
@@ -451,12 +512,12 @@ template <typename R> class Davidson {
             if (nex > 0) {
                 const T* B = V_ + (size_t)start * npw_;
                 const T* SB = SV_ + (size_t)start * npw_;
-                gemm(true, nex, 1, npw_, one(), B, npw_, sv, npw_, zero(), coef_, nex);
+                inner(nex, 1, B, sv, coef_, nex);
                 gemm(false, npw_, 1, nex, mone(), B, npw_, coef_, nex, one(), v, npw_);
                 gemm(false, npw_, 1, nex, mone(), SB, npw_, coef_, nex, one(), sv, npw_);
             }
             // ||v||_S^2 = Re v^H S v
-            gemm(true, 1, 1, npw_, one(), v, npw_, sv, npw_, zero(), coef_, 1);
+            inner(1, 1, v, sv, coef_, 1);
             T* hb = static_cast<T*>(host_readback(sizeof(T)));
             Q3B_CUDA(cudaMemcpyAsync(hb, coef_, sizeof(T), cudaMemcpyDeviceToHost, st_));
             Q3B_CUDA(cudaStreamSynchronize(st_));
@@ -475,7 +536,19 @@ template <typename R> class Davidson {
 
     void apply(int first, int count) {
         if (count <= 0) return;
-        c_.apply_h<R>(V_ + (size_t)first * npw_, npw_, HV_ + (size_t)first * npw_, npw_, count);
+        if (gamma_) {
+            // two bands per full-sphere vector (hamiltonian_applicator/serial.hpp:283-418)
+            const int nfull = c_.kp.npw, np = (count + 1) / 2;
+            gamma_pack<T><<<gamma_blocks((long)npw_ * np), 256, 0, st_>>>(npw_, count, V_ + (size_t)first * npw_,
+                                                                         npw_, gphi_, nfull);
+            Q3B_LAUNCH_CHECK();
+            c_.apply_h<R>(gphi_, nfull, ghphi_, nfull, np);
+            gamma_unpack<T><<<gamma_blocks((long)npw_ * np), 256, 0, st_>>>(npw_, count, ghphi_, nfull,
+                                                                           HV_ + (size_t)first * npw_, npw_);
+            Q3B_LAUNCH_CHECK();
+        } else {
+            c_.apply_h<R>(V_ + (size_t)first * npw_, npw_, HV_ + (size_t)first * npw_, npw_, count);
+        }
         happly_ += count;
     }
 
@@ -645,7 +718,9 @@ template <typename R> class Davidson {
     int npw_, nb_, maxn_ = 0;
     int happly_ = 0;
     T *V_, *HV_, *SV_, *tmp_, *evecR_, *cpack_, *cneg_, *coef_, *uinvR_;
-    bool us_ = false;  // S is not the identity (ultrasoft overlap blocks set)
+    T *gphi_ = nullptr, *ghphi_ = nullptr;  // packed band pairs (Gamma-only)
+    bool us_ = false;     // S is not the identity (ultrasoft overlap blocks set)
+    bool gamma_ = false;  // half-sphere vectors of a Gamma-only k-point
     double2 *Hs_, *Ss_, *evec_, *gram_, *uinv_;
     double *w_, *eps_, *norms_;
     int* idx_;
@@ -662,7 +737,7 @@ template <typename R> class Davidson {
 void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, const q3b_davidson_opts& o,
                     q3b_davidson_stats* stats) {
     c.require_ready();
-    const int npw = c.kp.npw;
+    const int npw = c.band_npw();
     if (nb <= 0 || nb > npw) throw Status(Q3B_ERR_INVALID, "band count must be in [1, npw]");
     if (o.basis_expansion_factor < 2) throw Status(Q3B_ERR_INVALID, "basis_expansion_factor must be >= 2");
     if (!(o.tolerance > 0.0)) throw Status(Q3B_ERR_INVALID, "tolerance must be positive");

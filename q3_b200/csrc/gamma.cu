@@ -18,79 +18,15 @@
 // each band its own kinetic, local and nonlocal terms.  The origin is packed
 // as (Re a(0), Re b(0)) and read back as (Re, Im), as in the reference.  A last
 // band without a partner is packed alone (a at +G, conj(a) at -G, a(0) as is)
-// and read from +G, the reference's single-band path; its nonlocal term then
-// uses a(0) as given, where the reference takes Re a(0) (the two agree for a
-// state that is real in real space, whose a(0) is real).
+// and read from +G, the reference's single-band path (its origin read as the
+// real part); its nonlocal term then uses a(0) as given, where the reference
+// takes Re a(0) (the two agree for a state that is real in real space, whose
+// a(0) is real).
 #include "context.cuh"
+#include "gamma.cuh"
 #include "nonlocal.cuh"
 #include "q3b.h"
 
-namespace q3b {
-namespace {
-
-inline int grid_blocks(long n) {
-    long b = (n + 255) / 256;
-    if (b > 148L * 16) b = 148L * 16;
-    return static_cast<int>(b < 1 ? 1 : b);
-}
-
-// phi_p (pair p = bands 2p, 2p+1): +G of half index h at h, -G at nhalf-1+h
-__global__ void gamma_pack(int nhalf, int nvec, const double2* __restrict__ psi, long ldpsi,
-                           double2* __restrict__ phi, long ldphi) {
-    const int npair = (nvec + 1) / 2;
-    const long total = (long)nhalf * npair;
-    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-         idx += (long)gridDim.x * blockDim.x) {
-        const int h = static_cast<int>(idx % nhalf), p = static_cast<int>(idx / nhalf);
-        const int b1 = 2 * p, b2 = 2 * p + 1;
-        const double2 a = psi[h + (long)b1 * ldpsi];
-        double2* out = phi + (long)p * ldphi;
-        if (b2 < nvec) {
-            const double2 b = psi[h + (long)b2 * ldpsi];
-            if (h == 0) {
-                out[0] = mk(a.x, b.x);
-            } else {
-                out[h] = mk(a.x - b.y, a.y + b.x);               // a + i b
-                out[nhalf - 1 + h] = mk(a.x + b.y, b.x - a.y);   // conj(a) + i conj(b)
-            }
-        } else {
-            out[h] = a;
-            if (h > 0) out[nhalf - 1 + h] = conj2(a);
-        }
-    }
-}
-
-// separation: a += (F(+G) + conj F(-G)) / 2, b += -i (F(+G) - conj F(-G)) / 2;
-// at the origin (Re F, Im F); a band without a partner reads F(+G)
-__global__ void gamma_unpack(int nhalf, int nvec, const double2* __restrict__ F, long ldf,
-                             double2* __restrict__ hpsi, long ldh) {
-    const int npair = (nvec + 1) / 2;
-    const long total = (long)nhalf * npair;
-    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-         idx += (long)gridDim.x * blockDim.x) {
-        const int h = static_cast<int>(idx % nhalf), p = static_cast<int>(idx / nhalf);
-        const int b1 = 2 * p, b2 = 2 * p + 1;
-        const double2* f = F + (long)p * ldf;
-        const double2 fp = f[h];
-        if (b2 < nvec) {
-            if (h == 0) {
-                hpsi[(long)b1 * ldh] = mk(fp.x, 0.0);
-                hpsi[(long)b2 * ldh] = mk(fp.y, 0.0);
-            } else {
-                const double2 fm = conj2(f[nhalf - 1 + h]);
-                const double2 s = mk(0.5 * (fp.x + fm.x), 0.5 * (fp.y + fm.y));
-                const double2 d = mk(0.5 * (fp.x - fm.x), 0.5 * (fp.y - fm.y));
-                hpsi[h + (long)b1 * ldh] = s;
-                hpsi[h + (long)b2 * ldh] = mk(d.y, -d.x);
-            }
-        } else {
-            hpsi[h + (long)b1 * ldh] = fp;
-        }
-    }
-}
-
-}  // namespace
-}  // namespace q3b
 
 using q3b::Context;
 
@@ -160,7 +96,7 @@ int q3b_apply_h_gamma(q3b_context* ctx, const q3b_cplx128* psi, q3b_cplx128* hps
         double2* phi = c.ws_gamma.as<double2>();
         double2* hphi = phi + n;
         const long work = (long)nhalf * npair;
-        q3b::gamma_pack<<<q3b::grid_blocks(work), 256, 0, c.stream>>>(
+        q3b::gamma_pack<<<q3b::gamma_blocks(work), 256, 0, c.stream>>>(
             nhalf, nvec, reinterpret_cast<const double2*>(psi), nhalf, phi, nfull);
         Q3B_LAUNCH_CHECK();
         if (precision == Q3B_FP64) {
@@ -172,7 +108,7 @@ int q3b_apply_h_gamma(q3b_context* ctx, const q3b_cplx128* psi, q3b_cplx128* hps
             c.apply_h<float>(c.ws_conv_in.as<float2>(), nfull, c.ws_conv_out.as<float2>(), nfull, npair);
             q3b::convert<float, double>(c.stream, (long)n, c.ws_conv_out.as<float2>(), hphi);
         }
-        q3b::gamma_unpack<<<q3b::grid_blocks(work), 256, 0, c.stream>>>(
+        q3b::gamma_unpack<<<q3b::gamma_blocks(work), 256, 0, c.stream>>>(
             nhalf, nvec, hphi, nfull, reinterpret_cast<double2*>(hpsi), nhalf);
         Q3B_LAUNCH_CHECK();
     });
@@ -195,11 +131,11 @@ int q3b_apply_s_gamma(q3b_context* ctx, const q3b_cplx128* psi, q3b_cplx128* sps
         double2* phi = c.ws_gamma.as<double2>();
         double2* sphi = phi + n;
         const long work = (long)nhalf * npair;
-        q3b::gamma_pack<<<q3b::grid_blocks(work), 256, 0, c.stream>>>(
+        q3b::gamma_pack<<<q3b::gamma_blocks(work), 256, 0, c.stream>>>(
             nhalf, nvec, reinterpret_cast<const double2*>(psi), nhalf, phi, nfull);
         Q3B_LAUNCH_CHECK();
         q3b::apply_s_device(c, phi, sphi, npair, precision);
-        q3b::gamma_unpack<<<q3b::grid_blocks(work), 256, 0, c.stream>>>(
+        q3b::gamma_unpack<<<q3b::gamma_blocks(work), 256, 0, c.stream>>>(
             nhalf, nvec, sphi, nfull, reinterpret_cast<double2*>(spsi), nhalf);
         Q3B_LAUNCH_CHECK();
     });

@@ -240,3 +240,46 @@ def test_davidson_ultrasoft_generalized(cuda_device, ctx_app, precision):
 
 def odense(kp, sy):
     return ohpsi.dense_hamiltonian(kp, sy.v_r, sy.cell.grid)
+
+
+@pytest.mark.parametrize("precision,ultrasoft", [(FP64, False), (MIXED, False), (FP64, True)])
+def test_davidson_gamma_half_sphere(cuda_device, ctx_app, precision, ultrasoft):
+    """On a Gamma-only k-point the solve runs on half-sphere vectors (real inner products, two bands
+    per H application): its eigenvalues are the full-sphere spectrum, its bands orthonormal in the
+    half-sphere metric 2 Re(a^H b) - a_0 b_0 (S-orthonormal with overlap blocks)."""
+    import scipy.linalg as sl
+    from oracle import overlap as oov
+    from q3_b200.davidson import PlanewaveDavidsonDiagonalizer
+    sy = synthetic.small_system(nbands=5, grid=(12, 12, 12), a=7.0, ecut=8.0, natoms=2, seed=23)
+    kp = sy.kpoints[0]
+    g = synthetic.gamma_kpoint(sy)
+    ctx_app.update_potential(sy.v_r, sy.cell.grid)
+    ctx_app.prepare_kpoint_gamma(g.npw, g.g_to_grid, g.minus_g_to_grid, g.ke, g.beta, g.atom_proj_offsets,
+                                 g.d_blocks)
+    h = odense(kp, sy)
+    if ultrasoft:
+        q = synthetic.overlap_blocks(sy, scale=0.2)
+        ctx_app.set_overlap_blocks(q)
+        s = oov.apply_s(np.eye(kp.npw, dtype=complex), kp.beta, q, kp.atom_proj_offsets)
+        exact = sl.eigh(h, s, eigvals_only=True)[:sy.nbands]
+    else:
+        exact = np.linalg.eigvalsh(h)[:sy.nbands]
+    rng = np.random.default_rng(4)
+    psi = rng.standard_normal((g.npw, sy.nbands)) + 1j * rng.standard_normal((g.npw, sy.nbands))
+    psi[0] = psi[0].real
+    dv = PlanewaveDavidsonDiagonalizer(ctx_app, precision)
+    dv.set_tolerance(1e-11)
+    dv.set_maximum_iterations(200)
+    if precision == MIXED:
+        dv.set_precision(MIXED, refine_sweeps=200)
+    r = dv.solve(psi, sy.nbands)
+    assert r.unconverged == 0
+    assert np.max(np.abs(r.eigenvalues - exact)) < 1e-8
+    z = r.bands
+    if ultrasoft:
+        from oracle import overlap as oov2
+        sz = oov2.apply_s_gamma(z, g.beta, q, g.atom_proj_offsets)
+    else:
+        sz = z
+    gram = 2.0 * (z.conj().T @ sz).real - np.outer(z[0].conj(), sz[0]).real
+    assert np.max(np.abs(gram - np.eye(sy.nbands))) < 1e-8
