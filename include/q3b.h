@@ -192,7 +192,11 @@ typedef struct {
 
 void q3b_davidson_default_opts(q3b_davidson_opts* opts);
 
-/* Solve for the nb lowest eigenpairs at the prepared k-point.
+/* Solve for the nb lowest eigenpairs at the prepared k-point.  With overlap
+ * blocks set (q3b_set_overlap_blocks) the problem is H c = eps S c and the bands
+ * come back S-orthonormal; on a k-point prepared with q3b_prepare_kpoint_gamma
+ * the bands are half-sphere vectors (npw = npw_half) under the real inner
+ * product 2 Re(a^H b) - Re(conj(a_0) b_0).
  *   bands_host   npw x nb (ld npw): in, the starting bands (the reference seeds
  *                from the stored bands, davidson.hpp:1000-1045; zero columns are
  *                replaced by lowest-kinetic-energy plane waves, :1047-1101);
