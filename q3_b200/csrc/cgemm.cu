@@ -163,10 +163,10 @@ __global__ void splitk_reduce(int M, int N, int splits, const cplx_t<R>* __restr
     }
 }
 
-// Products whose 64x64 tiling leaves most SMs idle (the subspace eigensolver's
-// n x n x n products, n <= 256) run on 32x32 tiles: four times the blocks and
-// a quarter of the serial K loop per block.
-constexpr long kSmallTiles = 64;
+// Products whose 64x64 tiling has fewer tiles than the GPU has SMs (the
+// subspace eigensolver's n x n x n products up to n = 767) run on 32x32 tiles:
+// four times the blocks and a quarter of the serial K loop per block.
+constexpr long kSmallTiles = 148;
 inline bool small_tiles(int M, int N) { return (long)ceil_div(M, kBM) * ceil_div(N, kBN) < kSmallTiles; }
 
 // K splits for a product with `tiles` output tiles (never more than for
