@@ -562,7 +562,11 @@ def run_q3b(args):
     from q3_b200.plan_info import stick_count
     nsticks = stick_count(kp, sy.cell.grid)
     kb32 = kernel_bytes(kp, sy.cell.grid, nsticks, nb, 8, 4)
-    traffic = traffic_table().get(f"config1/{name}/fp32")
+    tt = traffic_table()
+    traffic = tt.get(f"config1/{name}/fp32")
+    if traffic is not None and tt.get(f"config1/{name}/fp32/bands"):
+        # the captured launch's traffic, scaled to this step's average launch
+        traffic = traffic * (nb / max(1, n_dom)) / tt[f"config1/{name}/fp32/bands"]
     if name in ("projector_overlap", "projector_accumulate"):
         fl = kernel_flops(kp, nb)[name]
         achieved = fl / (ms_dom * 1e-3) / 1e12
