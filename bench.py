@@ -53,10 +53,14 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=32)
     ap.add_argument("--serving-rate", type=float, default=0.0,
                     help="arrivals per second (default: 80%% of the measured FP64 capacity)")
-    ap.add_argument("--probe", choices=["mixed", "fp64", "hegv"], default=None,
+    ap.add_argument("--probe", choices=["mixed", "fp64", "hegv", "density"], default=None,
                     help="profiling aid: apply H to the bench block three times in one precision "
-                         "(after the plane-kernel tuning), or run the subspace eigensolver on "
-                         "random problems of the --hegv-orders (hegv), and exit; prints no bench line")
+                         "(after the plane-kernel tuning), run the subspace eigensolver on "
+                         "random problems of the --hegv-orders (hegv), or accumulate the charge "
+                         "density of --density-bands bands of the bench cell (density), and exit; "
+                         "prints no bench line")
+    ap.add_argument("--density-bands", type=int, default=39,
+                    help="bands for --probe density (39: one stick chunk of the 80^3 cell in FP64)")
     ap.add_argument("--hegv-orders", default="16,32,64,96,128,192,256,384,512",
                     help="orders for --probe hegv, comma separated")
     return ap.parse_args()
@@ -293,6 +297,115 @@ def warm_server(srv, jobs, prec):
         ids.append(srv.submit(sy, k=k, tolerance=1e-9, max_iterations=2, precision=prec))
     for i in ids:
         srv.wait(i)
+
+
+def next_rows_section(device):
+    """The steps either side of the hot path, each timed on the bench cell (config 1): the
+    starting-subspace rotation, the projector set built on the device against its upload, the
+    charge-density accumulation, and the Gamma-only H|psi>, S|psi> and Davidson iteration on
+    half-sphere vectors (two bands per transform).  Device-side calls are timed with CUDA events
+    on the library's stream, host calls by the wall clock around a synchronised call."""
+    import torch
+    from q3_b200 import synthetic
+    from q3_b200._lib import FP64, MIXED
+    from q3_b200.applicator import PlanewaveHamiltonianApplicator
+    from q3_b200.davidson import PlanewaveDavidsonDiagonalizer
+    from q3_b200.starting import rotate_starting_vectors
+    sy = synthetic.config(1)
+    kp = sy.kpoints[0]
+    nb = sy.nbands
+    dev = torch.device("cuda", device)
+    out = {}
+
+    def wall(fn, reps=3):
+        fn()
+        torch.cuda.synchronize(dev)
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize(dev)
+            ts.append(time.perf_counter() - t0)
+        return 1e3 * float(np.median(ts))
+
+    def events(ap, fn, reps=5):
+        stream = torch.cuda.ExternalStream(ap.ctx.stream, device=dev)
+        torch.cuda.synchronize(dev)
+        fn()
+        torch.cuda.synchronize(dev)
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    ap = PlanewaveHamiltonianApplicator(device=device)
+    ap.update_potential(sy.v_r, sy.cell.grid)
+    # projector set: built on the device from beta tables, against the upload of the matrix
+    kpg = (kp.miller + kp.k_frac[None, :]) @ sy.cell.reciprocal
+    pos = sy.cell.positions_frac @ sy.cell.lattice
+    dq = 0.01
+    qg = np.arange(0.0, float(np.max(np.linalg.norm(kpg, axis=1))) + 5 * dq, dq)
+    tables = np.array([synthetic._radial_transform(l, qg) for (l, _ch) in synthetic.CHANNELS])
+    beta_l = [[l for (l, _ch) in synthetic.CHANNELS]]
+    species = np.zeros(pos.shape[0], dtype=np.int32)
+    out["projectors_built_ms"] = wall(lambda: ap.prepare_kpoint_build(
+        0, kp.npw, kp.g_to_grid, kp.ke, kpg, sy.cell.volume, pos, species, beta_l, tables, dq, kp.d_blocks))
+    out["projectors_uploaded_ms"] = wall(lambda: ap.prepare_system_kpoint(sy))
+    out["projector_matrix_bytes"] = int(kp.npw * kp.nproj * 16)
+    # starting subspace: 5/4 nb random vectors rotated to nb bands (H chi, chi^H H chi, zhegv, chi c)
+    nchi = nb + nb // 4
+    rng = np.random.default_rng(7)
+    chi = np.asfortranarray(rng.standard_normal((kp.npw, nchi)) + 1j * rng.standard_normal((kp.npw, nchi)))
+    out["starting_subspace_ms"] = wall(lambda: rotate_starting_vectors(ap, chi, nb))
+    out["starting_subspace_vectors"] = nchi
+    out["starting_subspace_upload_bytes"] = int(chi.nbytes)
+    # charge density of the nb bands
+    psi = torch.from_numpy(np.ascontiguousarray(sy.psi0[0].T)).to(dev)
+    rho = torch.zeros(int(np.prod(sy.cell.grid)), dtype=torch.float64, device=dev)
+    w = np.full(nb, 2.0 / sy.cell.volume)
+    ms = events(ap, lambda: ap.accumulate_density(psi, w, rho))
+    out["density_ms"] = ms
+    out["density_bands_per_s"] = nb / (ms * 1e-3)
+    ap.ctx.close()
+    # Gamma-only: the same cell on the half sphere
+    g = synthetic.gamma_kpoint(sy)
+    ag = PlanewaveHamiltonianApplicator(device=device)
+    ag.update_potential(sy.v_r, sy.cell.grid)
+    ag.prepare_kpoint_gamma(g.npw, g.g_to_grid, g.minus_g_to_grid, g.ke, g.beta, g.atom_proj_offsets, g.d_blocks)
+    ph = rng.standard_normal((g.npw, nb)) + 1j * rng.standard_normal((g.npw, nb))
+    ph[0] = ph[0].real
+    x = torch.from_numpy(np.ascontiguousarray(ph.T)).to(dev)
+    y = torch.empty_like(x)
+    gam = {"npw_half": g.npw, "bands": nb}
+    for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+        ms = events(ag, lambda: ag.lib.q3b_apply_h_gamma(ag.h, x.data_ptr(), y.data_ptr(), nb, prec))
+        gam[f"hpsi_{name}_band_applications_per_s"] = nb / (ms * 1e-3)
+    ag.set_overlap_blocks(synthetic.overlap_blocks(sy))
+    for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+        ms = events(ag, lambda: ag.lib.q3b_apply_s_gamma(ag.h, x.data_ptr(), y.data_ptr(), nb, prec))
+        gam[f"spsi_{name}_band_applications_per_s"] = nb / (ms * 1e-3)
+    ag.prepare_kpoint_gamma(g.npw, g.g_to_grid, g.minus_g_to_grid, g.ke, g.beta, g.atom_proj_offsets, g.d_blocks)
+    it = 6
+    for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+        d = PlanewaveDavidsonDiagonalizer(ag, prec)
+        d.set_tolerance(1e-14)
+        if prec == MIXED:
+            d.set_precision(MIXED, 1e-14, 1)
+        d.set_maximum_iterations(1)
+        d.solve(x.clone(), nb)
+        d.set_maximum_iterations(it)
+        r = d.solve(x.clone(), nb)
+        phase_s = r.seconds - (r.fp64_seconds if prec == MIXED else 0.0)
+        phase_it = r.iterations - (r.fp64_iterations if prec == MIXED else 0)
+        gam[f"davidson_iteration_ms_{name}"] = 1e3 * phase_s / max(1, phase_it)
+    out["gamma_only"] = gam
+    ag.ctx.close()
+    return out
 
 
 def davidson_section(ap, sy1, psi64, args):
@@ -546,8 +659,10 @@ def run_q3b(args):
 
     # Davidson: per iteration on this cell; converged solves on the other configs
     dav = None
+    nxt = None
     if not args.no_davidson:
         dav = davidson_section(ap, sy, psi64, args)
+        nxt = next_rows_section(local) if rank == 0 else None
 
     if rank != 0:
         if pg is not None:
@@ -610,6 +725,7 @@ def run_q3b(args):
         "gpu_launches": launches,
         "clocks": cs,
         "davidson": dav,
+        "next_rows": nxt,
     }
     print(json.dumps(line), flush=True)
     if pg is not None:
@@ -653,11 +769,44 @@ def run_hegv_probe(args):
     print(json.dumps({"probe": "hegv", "ms": out}), flush=True)
 
 
+def run_density_probe(args):
+    """Charge density of the first --density-bands bands of the 64-atom cell: three untimed
+    calls, then five timed by CUDA events on the library's stream (median printed)."""
+    import torch
+    from q3_b200 import synthetic
+    from q3_b200.applicator import PlanewaveHamiltonianApplicator
+    sy = synthetic.config(1)
+    ap = PlanewaveHamiltonianApplicator()
+    ap.update_potential(sy.v_r, sy.cell.grid)
+    ap.prepare_system_kpoint(sy)
+    nb = max(1, min(int(args.density_bands), sy.nbands))
+    dev = torch.device("cuda", ap.ctx.device)
+    psi = torch.from_numpy(np.ascontiguousarray(sy.psi0[0][:, :nb].T)).to(dev)
+    rho = torch.zeros(int(np.prod(sy.cell.grid)), dtype=torch.float64, device=dev)
+    w = np.full(nb, 2.0 / sy.cell.volume)
+    stream = torch.cuda.ExternalStream(ap.ctx.stream, device=dev)
+    for _ in range(3):
+        ap.accumulate_density(psi, w, rho)
+    torch.cuda.synchronize(dev)
+    ts = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ap.accumulate_density(psi, w, rho)
+        e1.record(stream)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    print(json.dumps({"probe": "density", "bands": nb, "ms": float(np.median(ts))}), flush=True)
+
+
 def run_probe(args):
     """Three H|psi> applications of the bench block in one precision: a short,
     fixed launch sequence for ncu captures of the plane and GEMM kernels."""
     if args.probe == "hegv":
         run_hegv_probe(args)
+        return
+    if args.probe == "density":
+        run_density_probe(args)
         return
     import torch
     from q3_b200 import synthetic

@@ -209,14 +209,14 @@ int q3b_accumulate_density(q3b_context* ctx, const q3b_cplx128* psi, int nvec, c
         if (nvec < 0 || (nvec > 0 && (!psi || !weights || !rho))) throw q3b::Status(Q3B_ERR_INVALID, "bad arguments");
         if (nvec == 0) return;
         const q3b::LocalPlan<double>& lp = c.local_plan<double>();
-        const int groups = q3b::density_groups(lp, nvec);
+        const int chunk = c.sticks_chunk<double>(nvec);
+        const int groups = q3b::density_groups(lp, chunk);
         const size_t n = (size_t)lp.n1 * lp.n2 * lp.n3;
         const size_t pbytes = ((groups * n * sizeof(double)) + 255) & ~size_t(255);
         c.ws_density.reserve(&c, pbytes + (size_t)nvec * sizeof(double));
         double* partial = c.ws_density.as<double>();
         double* w = reinterpret_cast<double*>(c.ws_density.as<char>() + pbytes);
-        Q3B_CUDA(cudaMemcpyAsync(w, weights, (size_t)nvec * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-        const int chunk = c.sticks_chunk<double>(nvec);
+        q3b::upload_async(w, weights, (size_t)nvec * sizeof(double), c.stream);
         c.ws_sticks.reserve(&c, (size_t)chunk * q3b::sticks_bytes_per_band(lp));
         q3b::accumulate_density(c.stream, lp, reinterpret_cast<const double2*>(psi), c.kp.npw, nvec, w,
                                 c.ws_sticks.as<double2>(), chunk, partial, groups, rho);

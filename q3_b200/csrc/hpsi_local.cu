@@ -252,8 +252,10 @@ void launch_planes(dim3 grid, size_t smem, cudaStream_t st, const LocalPlan<R>& 
 // left in digit-reversed order) and adds w_b |psi(r)|^2 into its own slab of
 // `partial` ([g][i3][w1 pos][w2 pos]); one block per slab, bands in order, so
 // the sums are deterministic.  Bands of weight 0 are skipped.
+constexpr int kAccBatch = 16;
+
 template <int MAXR>
-__global__ void __launch_bounds__(256) planes_density(LocalPlan<double> p, const double2* X, int nb,
+__global__ void __launch_bounds__(256, 2) planes_density(LocalPlan<double> p, const double2* X, int nb,
                                                       const double* w, double* partial, int groups) {
     using T = double2;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -285,9 +287,24 @@ __global__ void __launch_bounds__(256) planes_density(LocalPlan<double> p, const
         __syncthreads();
         fft::run_b<+1, MAXR>(plane, gc, tw1);
         __syncthreads();
-        for (int i = threadIdx.x; i < nplane; i += blockDim.x) {
-            const T v = plane[(i / p.n2) * p.p2 + i % p.n2];
-            acc[i] += wb * (v.x * v.x + v.y * v.y);
+        // the slab's loads are issued kAccBatch at a time, so that as many are
+        // in flight per thread rather than one load's latency per position
+        for (int i0 = threadIdx.x; i0 < nplane; i0 += kAccBatch * blockDim.x) {
+            double old[kAccBatch];
+#pragma unroll
+            for (int j = 0; j < kAccBatch; ++j) {
+                const int i = i0 + j * blockDim.x;
+                old[j] = i < nplane ? acc[i] : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < kAccBatch; ++j) {
+                const int i = i0 + j * blockDim.x;
+                if (i < nplane) {
+                    const int row = i / p.n2;
+                    const T v = plane[row * p.p2 + (i - row * p.n2)];
+                    acc[i] = old[j] + wb * (v.x * v.x + v.y * v.y);
+                }
+            }
         }
         __syncthreads();
     }
@@ -403,27 +420,72 @@ void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, l
     }
 }
 
+namespace {
+
+// the partial slabs of the density stay below this many bytes, so that they
+// stay in L2 beside a stick chunk (48 MB) while the bands add into them
+constexpr size_t kDensityPartialBytes = 32ull << 20;
+
+bool density_small_factors(const LocalPlan<double>& p) {
+    return p.na1 <= kSmallR && p.nb1 <= kSmallR && p.na2 <= kSmallR && p.nb2 <= kSmallR;
+}
+
+void set_density_limits() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaFuncSetAttribute(planes_density<kSmallR>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(planes_density<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    });
+}
+
+}  // namespace
+
+// A density block runs its group's bands one after another on one plane, so a
+// launch of n3 * groups blocks takes ceil(n3 * groups / resident blocks) waves
+// of ceil(nvec / groups) band-planes each.  The group count is the one that
+// minimises that product (the smallest on a tie), within the slab budget: on
+// an 80^3 grid with two resident blocks per SM, a 39-band chunk runs as 7
+// groups of 6 bands in 2 waves (12 band-planes a block), where 4 groups of 10
+// would take 2 waves of 10 band-planes, the second with 24 blocks on 148 SMs.
 int density_groups(const LocalPlan<double>& p, int nvec) {
-    int g = (2 * 148 + p.n3 - 1) / p.n3;
-    if (g > nvec) g = nvec;
-    return g < 1 ? 1 : g;
+    if (nvec < 1) return 1;
+    set_density_limits();
+    int per_sm = 0, dev = 0, sms = 0;
+    if (density_small_factors(p))
+        Q3B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, planes_density<kSmallR>, 256,
+                                                               plane_smem_bytes(p)));
+    else
+        Q3B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, planes_density<16>, 256, plane_smem_bytes(p)));
+    Q3B_CUDA(cudaGetDevice(&dev));
+    Q3B_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long slots = (long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+    const size_t slab = (size_t)p.n1 * p.n2 * p.n3 * sizeof(double);
+    long gmax = static_cast<long>(kDensityPartialBytes / slab);
+    if (gmax > nvec) gmax = nvec;
+    if (gmax < 1) gmax = 1;
+    int best = 1;
+    long best_cost = -1;
+    for (int g = 1; g <= gmax; ++g) {
+        const long cost = (long)ceil_div((long)p.n3 * g, slots) * ceil_div(nvec, g);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = g;
+        }
+    }
+    return best;
 }
 
 void accumulate_density(cudaStream_t st, const LocalPlan<double>& p, const double2* psi, long ldpsi, int nvec,
                         const double* w, double2* X, int chunk, double* partial, int groups, double* rho) {
     if (nvec <= 0 || p.nsticks == 0) return;
     set_smem_limits<double>();
-    static std::once_flag once;
-    std::call_once(once, [] {
-        cudaFuncSetAttribute(planes_density<kSmallR>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(planes_density<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    });
+    set_density_limits();
     if (chunk < 1) chunk = 1;
     const size_t smem_s = stick_smem_bytes(p);
     const size_t smem_p = plane_smem_bytes(p);
     const int nsg = ceil_div(p.nsticks, p.sg);
     const bool small3 = p.na3 <= kSmallR && p.nb3 <= kSmallR;
-    const bool small12 = p.na1 <= kSmallR && p.nb1 <= kSmallR && p.na2 <= kSmallR && p.nb2 <= kSmallR;
+    const bool small12 = density_small_factors(p);
     Q3B_CUDA(cudaMemsetAsync(partial, 0, (size_t)groups * p.n1 * p.n2 * p.n3 * sizeof(double), st));
     for (int b0 = 0; b0 < nvec; b0 += chunk) {
         const int nb = nvec - b0 < chunk ? nvec - b0 : chunk;

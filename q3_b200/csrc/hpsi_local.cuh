@@ -75,7 +75,7 @@ void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, l
 // psi_b(r) the unnormalised backward transform of band b scattered onto the
 // grid.  w: nvec device weights (0 skips a band).  X: chunk *
 // sticks_bytes_per_band; partial: groups * N doubles with groups from
-// density_groups().
+// density_groups(p, chunk), the bands of one launch.
 int density_groups(const LocalPlan<double>& p, int nvec);
 void accumulate_density(cudaStream_t st, const LocalPlan<double>& p, const double2* psi, long ldpsi, int nvec,
                         const double* w, double2* X, int chunk, double* partial, int groups, double* rho);
