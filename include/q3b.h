@@ -173,6 +173,12 @@ typedef struct {
                                     the phase also ends once the change stops falling       */
     int profile_stages;          /* nonzero: fill q3b_davidson_stats.stage_ms (drains the
                                     stream at every stage boundary)                         */
+    double* eigenvalue_history;  /* optional host array of history_rows x nb (row-major): row
+                                    i = the nb Ritz values (Ry) of iteration i's subspace
+                                    solve, the FP32 phase's iterations first under MIXED;
+                                    rows past the iterations run are left as they are.  The
+                                    serving API ignores it.                                  */
+    int history_rows;            /* rows of eigenvalue_history (0: no history)              */
 } q3b_davidson_opts;
 
 typedef struct {

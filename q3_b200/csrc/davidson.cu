@@ -36,6 +36,7 @@ constexpr double kPrecondFloor = 1e-4;      // tolerances.hpp:50
 constexpr double kEmptyRelax = 5.0;         // tolerances.hpp:65
 constexpr double kEmptyFloor = 1e-5;        // tolerances.hpp:66
 constexpr double kStallBelow = 1e-5;        // Ry: the FP32 phase may stop on a plateau below this
+constexpr int kFlatIterations = 4;          // FP32 phase: iterations without a new band-energy low
 
 inline int grid_for(long n) {
     long b = (n + 255) / 256;
@@ -574,7 +575,13 @@ template <typename R> class Davidson {
     // stagnate: stop (with the Ritz pairs of this iteration) once the largest
     // eigenvalue change has stopped halving for three iterations while below
     // kStallBelow -- near the FP32 resolution of the eigenvalues, where the FP32
-    // phase of the mixed solve can go no further.
+    // phase of the mixed solve can go no further -- or once the sum of the
+    // occupied Ritz values has set no new low for kFlatIterations iterations.
+    // In exact arithmetic that sum never rises (the Ritz values fall as the
+    // basis grows and are kept across a collapse), so a sum that stops falling
+    // is the FP32 H|psi> accuracy floor (about 1e-4 Ry on the 80^3 and 108^3
+    // cells), below which further FP32 iterations leave the eigenvalues as
+    // they are.
     Result solve(int seeded, const std::vector<double>& stored, double tol, int max_it, int occupied,
                  T* out, bool want_resid, double* stage_ms = nullptr, bool stagnate = false) {
         Result res;
@@ -615,6 +622,8 @@ template <typename R> class Davidson {
             std::copy(dg.begin(), dg.end(), prev.begin());                // :488-494
         }
         const double empty_tol = std::max(kEmptyRelax * tol, kEmptyFloor);
+        double low = 0.0;
+        int since_low = 0;
         for (int it = 0; it < max_it; ++it) {                            // :498
             int info = 0;
             if (reuse_collapse_ && basis == nb_) {
@@ -638,6 +647,7 @@ template <typename R> class Davidson {
             }
             clk.stop(DIAG);
             ++res.iterations;
+            if (history_) history_->insert(history_->end(), whost_.begin(), whost_.begin() + nb_);
             std::vector<int> unconv;
             double maxchange = 0.0;
             for (int b = 0; b < nb_; ++b) {                               // :615-629
@@ -649,8 +659,17 @@ template <typename R> class Davidson {
             res.unconverged = static_cast<int>(unconv.size());
             if (it != 0) history.push_back(maxchange);
             const size_t h = history.size();
-            const bool stalled = stagnate && h >= 4 && history[h - 1] < kStallBelow &&
-                                 history[h - 1] > 0.5 * history[h - 4];
+            double occ_sum = 0.0;
+            for (int b = 0; b < occupied; ++b) occ_sum += whost_[b];
+            if (it == 0 || occ_sum < low) {
+                low = occ_sum;
+                since_low = 0;
+            } else {
+                ++since_low;
+            }
+            const bool stalled = stagnate && ((h >= 4 && history[h - 1] < kStallBelow &&
+                                               history[h - 1] > 0.5 * history[h - 4]) ||
+                                              since_low >= kFlatIterations);
             if (unconv.empty() || stalled) {                              // :649-668
                 res.stagnated = stalled && !unconv.empty();
                 extract(basis, out, want_resid ? &res.resid : nullptr);
@@ -694,6 +713,9 @@ template <typename R> class Davidson {
 
     int happly() const { return happly_; }
 
+    // keep the Ritz values of every iteration (nb per iteration) in *h
+    void record_history(std::vector<double>* h) { history_ = h; }
+
   private:
     void widen(int M, int N, const T* src, int lds, double2* dst, int ldd) {
         widen_block<R><<<grid_for((long)M * N), 256, 0, st_>>>(M, N, src, lds, dst, ldd);
@@ -727,6 +749,7 @@ template <typename R> class Davidson {
     const double* ke_;
     dense::Scratch dscratch_;
     std::vector<double> whost_;
+    std::vector<double>* history_ = nullptr;
     std::vector<double> collapse_w_;
     std::vector<double> wread_;  // eigenvalues of the last subspace solve, on the host
     bool reuse_collapse_ = false;
@@ -746,8 +769,13 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
     std::vector<double> stored(eig_host, eig_host + nb);
     q3b_davidson_stats s{};
     const size_t band_bytes = (size_t)npw * nb * sizeof(double2);
+    if (o.history_rows < 0 || (o.history_rows > 0 && !o.eigenvalue_history))
+        throw Status(Q3B_ERR_INVALID, "eigenvalue_history needs history_rows >= 0 and a buffer");
+    std::vector<double> hist;
+    std::vector<double>* rec = o.history_rows > 0 ? &hist : nullptr;
     if (o.precision == Q3B_FP64) {
         Davidson<double> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
+        dv.record_history(rec);
         Q3B_CUDA(cudaMemcpyAsync(dv.V(), bands_dev, band_bytes, cudaMemcpyDeviceToDevice, c.stream));
         auto r = dv.solve(nb, stored, o.tolerance, std::max(1, o.max_iterations), occupied, bands_dev, true,
                           o.profile_stages ? s.stage_ms : nullptr);
@@ -765,6 +793,7 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         int it32 = 0, h32 = 0, col32 = 0;
         {
             Davidson<float> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
+            dv.record_history(rec);
             convert<double, float>(c.stream, (long)npw * nb, bands_dev, dv.V());
             const double tol32 = o.mixed_tolerance > 0.0 ? o.mixed_tolerance : 1e-6;
             auto r = dv.solve(nb, stored, std::max(tol32, o.tolerance), std::max(1, o.max_iterations),
@@ -779,6 +808,7 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         // FP64 refinement sweeps from the FP32 Ritz pairs
         const auto t64 = std::chrono::steady_clock::now();
         Davidson<double> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
+        dv.record_history(rec);
         Q3B_CUDA(cudaMemcpyAsync(dv.V(), bands_dev, band_bytes, cudaMemcpyDeviceToDevice, c.stream));
         const int sweeps = o.refine_sweeps > 0 ? o.refine_sweeps : 6;
         auto r = dv.solve(nb, eig32, o.tolerance, sweeps, occupied, bands_dev, true,
@@ -798,6 +828,10 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
     Q3B_CUDA(cudaStreamSynchronize(c.stream));
     tc::check_error(c.stream);
     s.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (rec) {
+        const size_t rows = std::min(hist.size() / (size_t)nb, (size_t)o.history_rows);
+        std::copy(hist.begin(), hist.begin() + rows * nb, o.eigenvalue_history);
+    }
     if (stats) *stats = s;
 }
 

@@ -269,6 +269,8 @@ int q3b_server_submit(q3b_server* s, const q3b_request* r, int* id_out) {
         if (r->eigenvalues) j->eig.assign(r->eigenvalues, r->eigenvalues + r->nb);
         if (r->opts) j->opts = *r->opts;
         else q3b_davidson_default_opts(&j->opts);
+        j->opts.eigenvalue_history = nullptr;  // the caller's buffer is not written from a worker
+        j->opts.history_rows = 0;
         *id_out = s->impl->submit(std::move(j));
         return Q3B_OK;
     } catch (const std::exception& e) {

@@ -31,6 +31,7 @@ class SolveResult:
     seconds: float
     stage_ms: dict
     fp64_seconds: float
+    eigenvalue_history: Optional[np.ndarray] = None  # iterations x nb Ritz values (Ry), when kept
 
 
 class PlanewaveDavidsonDiagonalizer:
@@ -40,6 +41,7 @@ class PlanewaveDavidsonDiagonalizer:
         self.opts = DavidsonOpts()
         self.lib.q3b_davidson_default_opts(C.byref(self.opts))
         self.opts.precision = int(precision)
+        self.history_rows = 0
 
     def set_tolerance(self, tolerance: float) -> None:
         self.opts.tolerance = float(tolerance)
@@ -65,6 +67,11 @@ class PlanewaveDavidsonDiagonalizer:
     def set_profile_stages(self, on: bool = True) -> None:
         self.opts.profile_stages = 1 if on else 0
 
+    def set_eigenvalue_history(self, rows: int) -> None:
+        """Keep the Ritz values of up to `rows` iterations (both phases of a mixed solve) in
+        SolveResult.eigenvalue_history; 0 turns it off."""
+        self.history_rows = max(0, int(rows))
+
     def solve(self, bands, number_of_bands: int,
               stored_eigenvalues: Optional[np.ndarray] = None) -> SolveResult:
         """bands: npw x nb numpy array (host) or a torch complex128 CUDA tensor
@@ -74,6 +81,10 @@ class PlanewaveDavidsonDiagonalizer:
             np.ascontiguousarray(stored_eigenvalues, dtype=np.float64).copy()
         st = DavidsonStats()
         h = self.ap.h
+        rows = self.history_rows
+        hist = np.zeros((rows, nb), dtype=np.float64) if rows else None
+        self.opts.eigenvalue_history = hist.ctypes.data if rows else None
+        self.opts.history_rows = rows
         if isinstance(bands, np.ndarray):
             x = np.asfortranarray(bands, dtype=np.complex128).copy(order="F")
             rc = self.lib.q3b_davidson_solve(h, x.ctypes.data, eig.ctypes.data, nb,
@@ -86,9 +97,11 @@ class PlanewaveDavidsonDiagonalizer:
             out = bands
         check(h, rc)
         stages = dict(zip(DavidsonStats.STAGES, list(st.stage_ms)))
+        if hist is not None:
+            hist = hist[:min(rows, st.iterations)].copy()
         return SolveResult(eig, out, st.iterations, st.fp64_iterations, st.h_applications,
                            st.unconverged, st.collapses, st.max_residual_norm, st.seconds, stages,
-                           st.fp64_seconds)
+                           st.fp64_seconds, hist)
 
 
 def hegv(applicator, h: np.ndarray, s: np.ndarray):

@@ -283,3 +283,34 @@ def test_davidson_gamma_half_sphere(cuda_device, ctx_app, precision, ultrasoft):
         sz = z
     gram = 2.0 * (z.conj().T @ sz).real - np.outer(z[0].conj(), sz[0]).real
     assert np.max(np.abs(gram - np.eye(sy.nbands))) < 1e-8
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+def test_davidson_eigenvalue_history(cuda_device, ctx_app, precision):
+    """The per-iteration Ritz values: one row per iteration (the FP32 phase's rows first under
+    MIXED), the last row the returned eigenvalues of a converged solve, and rows that approach
+    the golden eigenvalues; a buffer shorter than the iterations keeps the first rows."""
+    from q3_b200.davidson import PlanewaveDavidsonDiagonalizer
+    g = np.load(Path(__file__).parent / "golden" / "config0_davidson.npz")
+    sy = synthetic.config(0)
+    _prep(ctx_app, sy)
+    d = PlanewaveDavidsonDiagonalizer(ctx_app, precision)
+    d.set_tolerance(1e-10)
+    d.set_maximum_iterations(100)
+    if precision == MIXED:
+        d.set_precision(MIXED, 1e-5, 30)
+    d.set_eigenvalue_history(200)
+    r = d.solve(sy.psi0[0], sy.nbands)
+    assert r.unconverged == 0
+    h = r.eigenvalue_history
+    assert h.shape == (r.iterations, sy.nbands)
+    assert np.array_equal(h[-1], r.eigenvalues)
+    err = np.max(np.abs(h - g["eigenvalues"][None, :]), axis=1)
+    assert err[-1] < (FP64_EIG_TOL_RY if precision == FP64 else MIXED_EIG_TOL_RY)
+    assert err[0] > 100 * err[-1]
+    if precision == MIXED:
+        assert r.fp64_iterations < r.iterations
+    d.set_eigenvalue_history(3)
+    r3 = d.solve(sy.psi0[0], sy.nbands)
+    assert r3.eigenvalue_history.shape == (3, sy.nbands)
+    assert np.max(np.abs(r3.eigenvalue_history - h[:3])) < 1e-9
