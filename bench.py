@@ -724,9 +724,11 @@ def run_q3b(args):
     # Davidson: per iteration on this cell; converged solves on the other configs
     dav = None
     nxt = None
+    study = None
     if not args.no_davidson:
         dav = davidson_section(ap, sy, psi64, args)
         nxt = next_rows_section(local) if rank == 0 else None
+        study = precision_study_section(local) if rank == 0 else None
 
     if rank != 0:
         if pg is not None:
@@ -790,6 +792,7 @@ def run_q3b(args):
         "clocks": cs,
         "davidson": dav,
         "next_rows": nxt,
+        "precision_study": study,
     }
     print(json.dumps(line), flush=True)
     if pg is not None:
