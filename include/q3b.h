@@ -168,7 +168,8 @@ typedef struct {
     int basis_expansion_factor;  /* set_basis_expansion_factor (davidson.hpp:260-264), >= 2 */
     int occupied_bands;          /* bands held to `tolerance`; the rest to max(5 tol, 1e-5)  */
     int precision;               /* Q3B_FP64 or Q3B_MIXED                                   */
-    int refine_sweeps;           /* MIXED: max FP64 refinement iterations at the end         */
+    int refine_sweeps;           /* MIXED: max FP64 refinement iterations at the end; 0 (the
+                                    default) allows max_iterations of them                   */
     double mixed_tolerance;      /* MIXED: eigenvalue-change tolerance of the FP32 phase, Ry;
                                     the phase also ends once the change stops falling       */
     int profile_stages;          /* nonzero: fill q3b_davidson_stats.stage_ms (drains the

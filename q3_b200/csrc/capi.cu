@@ -278,7 +278,7 @@ void q3b_davidson_default_opts(q3b_davidson_opts* o) {
     o->basis_expansion_factor = 2; // davidson.hpp:864
     o->occupied_bands = 0;         // 0: every band is occupied
     o->precision = Q3B_FP64;
-    o->refine_sweeps = 30;
+    o->refine_sweeps = 0;          // MIXED: refinement up to max_iterations
     o->mixed_tolerance = 1e-6;
     o->profile_stages = 0;
     o->eigenvalue_history = nullptr;

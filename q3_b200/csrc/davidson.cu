@@ -810,7 +810,7 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         Davidson<double> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
         dv.record_history(rec);
         Q3B_CUDA(cudaMemcpyAsync(dv.V(), bands_dev, band_bytes, cudaMemcpyDeviceToDevice, c.stream));
-        const int sweeps = o.refine_sweeps > 0 ? o.refine_sweeps : 6;
+        const int sweeps = o.refine_sweeps > 0 ? o.refine_sweeps : std::max(1, o.max_iterations);
         auto r = dv.solve(nb, eig32, o.tolerance, sweeps, occupied, bands_dev, true,
                           o.profile_stages ? s.stage_ms : nullptr);
         std::copy(r.eig.begin(), r.eig.end(), eig_host);

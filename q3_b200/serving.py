@@ -60,9 +60,10 @@ class BandSolveServer:
             raise _lib.Q3BError(rc, msg.decode() if msg else "")
 
     def submit(self, system, k: int = 0, tolerance: float = 1e-8, max_iterations: int = 100,
-               precision: int = FP64, mixed_tolerance: float = 1e-6, refine_sweeps: int = 100,
+               precision: int = FP64, mixed_tolerance: float = 1e-6, refine_sweeps: int = 0,
                bands: Optional[np.ndarray] = None) -> int:
-        """Queue one band solve of `system` at k-point `k`; returns its id."""
+        """Queue one band solve of `system` at k-point `k`; returns its id.  refine_sweeps 0
+        gives a mixed solve's FP64 refinement up to max_iterations iterations."""
         kp = system.kpoints[k]
         n1, n2, n3 = system.cell.grid
         v = np.ascontiguousarray(system.v_r, dtype=np.float64)

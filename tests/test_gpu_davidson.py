@@ -314,3 +314,22 @@ def test_davidson_eigenvalue_history(cuda_device, ctx_app, precision):
     r3 = d.solve(sy.psi0[0], sy.nbands)
     assert r3.eigenvalue_history.shape == (3, sy.nbands)
     assert np.max(np.abs(r3.eigenvalue_history - h[:3])) < 1e-9
+
+
+def test_mixed_default_refinement_converges_slow_request(cuda_device, ctx_app):
+    """Request 18 of the serving stream (112 bands, npw 11,123, 60^3) needs 207 FP64 iterations;
+    its mixed solve needs over 100 refinement iterations.  With the default refinement budget (up
+    to max_iterations) it converges, within 1e-8 Ha of the FP64 solve."""
+    from q3_b200.davidson import PlanewaveDavidsonDiagonalizer
+    sy = synthetic.serving_requests(19)[18]
+    _prep(ctx_app, sy)
+    res = {}
+    for prec in (FP64, MIXED):
+        d = PlanewaveDavidsonDiagonalizer(ctx_app, prec)
+        d.set_tolerance(1e-9)
+        d.set_maximum_iterations(300)
+        res[prec] = d.solve(sy.psi0[0], sy.nbands)
+    assert res[FP64].unconverged == 0
+    assert res[MIXED].unconverged == 0
+    assert res[MIXED].iterations - res[MIXED].fp64_iterations > 0
+    assert np.max(np.abs(res[MIXED].eigenvalues - res[FP64].eigenvalues)) < MIXED_EIG_TOL_RY
