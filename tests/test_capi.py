@@ -42,3 +42,21 @@ def test_context_create_without_gpu_fails_cleanly():
     h = C.c_void_p()
     rc = lib.q3b_context_create(0, 0, C.byref(h))
     assert rc == _lib.ERR_CUDA and not h.value
+
+
+def test_davidson_default_opts_fill_every_field():
+    """q3b_davidson_default_opts is host code: it fills the ctypes mirror of q3b_davidson_opts
+    field by field, so a field order or size that differs from the header shows up here."""
+    import ctypes as C
+    from q3_b200 import _lib
+    lib = _lib.load()
+    o = _lib.DavidsonOpts()
+    o.tolerance, o.max_iterations, o.basis_expansion_factor = -1.0, -1, -1
+    o.occupied_bands, o.precision, o.refine_sweeps = -1, -1, -1
+    o.mixed_tolerance, o.profile_stages = -1.0, -1
+    o.eigenvalue_history, o.history_rows = 0x1234, 77
+    lib.q3b_davidson_default_opts(C.byref(o))
+    assert o.tolerance == 1e-2 and o.max_iterations == 20 and o.basis_expansion_factor == 2
+    assert o.occupied_bands == 0 and o.precision == _lib.FP64 and o.refine_sweeps == 0
+    assert o.mixed_tolerance == 1e-6 and o.profile_stages == 0
+    assert not o.eigenvalue_history and o.history_rows == 0
