@@ -109,8 +109,8 @@ int q3b_apply_h_host(q3b_context* ctx, const q3b_cplx128* psi_host, q3b_cplx128*
                      int nvec, int precision);
 
 /* q3b_apply_h (FP64) for callers that cannot allocate device memory during the
- * call: code inside a CUDA stream capture, runtimes that own all device memory
- * through their own pool, or that forbid allocation once started.  No
+ * call: runtimes that own all device memory through their own pool, or that
+ * forbid allocation once started.  No
  * counterpart in the reference.  Its scratch (the stick buffer and the
  * projector coefficients) is one fixed 32 MiB __device__ array that every GPU
  * loading the library holds until exit; bands are processed in batches that

@@ -1,8 +1,8 @@
 // q3b_apply_h_noalloc: FP64 H|psi> that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc while they apply H: code running inside
-// a CUDA stream capture or a device-memory pool they own, and runtimes that
-// forbid allocation after start-up.  This entry point serves them.  Its
+// Some callers cannot call cudaMalloc while they apply H: runtimes that own
+// all device memory through a pool of their own, and runtimes that forbid
+// allocation after start-up.  This entry point serves them.  Its
 // scratch -- the stick buffer of the sticks/planes transform and the two
 // projector-coefficient blocks of the nonlocal term -- lives in one
 // file-scope __device__ array of kNoallocScratchBytes (32 MiB), which every

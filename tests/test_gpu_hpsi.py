@@ -83,9 +83,9 @@ def test_hpsi_config0_golden(cuda_device):
     assert _rel(got, g["hpsi"]) < FP64_TOL
 
 
-def test_hpsi_config1_subset(cuda_device):
-    # the 64-atom 80^3 cell with 512 projectors, 24 bands
-    sy = synthetic.config(1, nbands=24)
+def test_hpsi_config1_all_bands(cuda_device):
+    # the 64-atom 80^3 cell with 512 projectors, the whole 256-band block
+    sy = synthetic.config(1)
     kp = sy.kpoints[0]
     ap = _applicator(sy)
     psi = sy.psi0[0]

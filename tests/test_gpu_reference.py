@@ -1,0 +1,160 @@
+"""The CUDA path against the reference's own CPU code, on the benchmark configurations.
+
+The fixtures (tests/golden/ref_config*.npz, made by tests/golden/make_ref_golden.py from the
+reference's compiled SerialPlanewaveHamiltonianApplicator, PlanewaveDavidsonDiagonalizer and
+SerialProjectorSetBuilder) fix the plane-wave order, the projector tables and the outputs;
+the potential and starting bands come from the seeded synthetic recipe.  The projector set
+enters the device either as the reference's own matrix (config 0, through
+q3b_prepare_kpoint) or built on the device from the reference's beta(q) tables
+(q3b_prepare_kpoint_build).
+
+Bars, in the units the reference works in (Ry):
+* FP64 H|psi>: 1e-12 relative to the largest entry (elements, Gram matrices, sketches);
+* FP32 H|psi> (mixed precision): 2e-5 relative;
+* FP64 Davidson: the same iteration count as the reference and eigenvalues within
+  2e-10 Ry (1e-10 Ha);
+* mixed Davidson: eigenvalues within 2e-8 Ry (1e-8 Ha) of the reference's FP64 solve.
+"""
+import numpy as np
+import pytest
+
+from q3_b200._lib import FP64, MIXED
+from tests.golden import ref_fixtures as RF
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+FP32_TOL = 2e-5
+FP64_EIG_TOL_RY = 2e-10
+MIXED_EIG_TOL_RY = 2e-8
+
+
+def _need(cid):
+    if not RF.path(cid).exists():
+        pytest.skip(f"{RF.path(cid).name} not generated")
+    return RF.load(cid)
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def _applicator():
+    from q3_b200.applicator import PlanewaveHamiltonianApplicator
+    return PlanewaveHamiltonianApplicator()
+
+
+def _apply(ap, psi, precision=FP64):
+    import torch
+    x = torch.from_numpy(np.asfortranarray(psi).T.copy()).to("cuda")
+    y = torch.empty_like(x)
+    ap.apply_batch(x, y, psi.shape[1], precision)
+    torch.cuda.synchronize()
+    return y.cpu().numpy().T
+
+
+def _solve(ap, psi0, nb, tol, max_it, precision=FP64, mixed_tol=1e-6):
+    from q3_b200.davidson import PlanewaveDavidsonDiagonalizer
+    dv = PlanewaveDavidsonDiagonalizer(ap, precision)
+    dv.set_tolerance(tol)
+    dv.set_maximum_iterations(max_it)
+    if precision == MIXED:
+        dv.set_precision(MIXED, mixed_tol, max_it)
+    return dv.solve(psi0, nb)
+
+
+# ------------------------------------------------------------------ config 0
+
+def _config0(ap, g, sy, rk, device_built=False):
+    if device_built:
+        RF.prepare_on_device(ap, sy, g, rk)
+    else:
+        ap.update_potential(sy.v_r, sy.cell.grid)
+        ap.prepare_kpoint(0, rk.npw, rk.g_to_grid, rk.ke, np.asfortranarray(g["beta"]),
+                          rk.atom_proj_offsets, rk.d_blocks)
+
+
+@pytest.mark.parametrize("device_built", [False, True], ids=["reference_matrix", "device_built"])
+def test_config0_hpsi(cuda_device, device_built):
+    g = _need(0)
+    sy = RF.system(0)
+    rk = RF.kpoint(sy, g)
+    ap = _applicator()
+    _config0(ap, g, sy, rk, device_built)
+    if device_built:
+        beta = ap.projectors().cpu().numpy().T
+        assert _rel(beta, g["beta"]) < 1e-13
+    assert _rel(_apply(ap, rk.psi0), g["hpsi"]) < FP64_TOL
+    assert _rel(_apply(ap, rk.psi0, MIXED), g["hpsi"]) < FP32_TOL
+
+
+def test_config0_davidson(cuda_device):
+    g = _need(0)
+    sy = RF.system(0)
+    rk = RF.kpoint(sy, g)
+    ap = _applicator()
+    _config0(ap, g, sy, rk)
+    got = _solve(ap, rk.psi0, sy.nbands, 1e-10, 200)
+    assert got.unconverged == int(g["unconverged_tol10"]) == 0
+    assert got.iterations == int(g["iterations_tol10"])
+    assert np.max(np.abs(got.eigenvalues - g["eig_tol10"])) < FP64_EIG_TOL_RY
+    mixed = _solve(ap, rk.psi0, sy.nbands, 1e-10, 200, MIXED)
+    assert mixed.unconverged == 0
+    assert np.max(np.abs(mixed.eigenvalues - g["eig_tol12"])) < MIXED_EIG_TOL_RY
+
+
+# ------------------------------------------------------- configs 1 and 3: H|psi>
+
+@pytest.mark.parametrize("cid", [1, 3])
+def test_large_cell_hpsi(cuda_device, cid):
+    g = _need(cid)
+    sy = RF.system(cid)
+    rk = RF.kpoint(sy, g)
+    ap = _applicator()
+    RF.prepare_on_device(ap, sy, g, rk)
+    psi = np.asfortranarray(rk.psi0[:, :RF.GRAM_BANDS])
+    s = RF.sketch_columns(rk.npw)
+    for precision, tol in ((FP64, FP64_TOL), (MIXED, FP32_TOL)):
+        h = _apply(ap, psi, precision)
+        assert _rel(h[:, 0], g["hpsi_band0"]) < tol
+        assert _rel(psi.conj().T @ h, g["gram_psi_hpsi"]) < tol
+        assert _rel(h.conj().T @ h, g["gram_hpsi_hpsi"]) < tol
+        assert _rel(s.conj().T @ h, g["sketch"]) < tol
+
+
+# ----------------------------------------------------- config 1: converged solve
+
+def test_config1_davidson(cuda_device):
+    g = _need(1)
+    sy = RF.system(1)
+    rk = RF.kpoint(sy, g)
+    ap = _applicator()
+    RF.prepare_on_device(ap, sy, g, rk)
+    got = _solve(ap, rk.psi0, sy.nbands, 1e-10, 300)
+    assert got.unconverged == int(g["unconverged_tol10"]) == 0
+    assert abs(got.iterations - int(g["iterations_tol10"])) <= 1
+    assert np.max(np.abs(got.eigenvalues - g["eig_tol10"])) < FP64_EIG_TOL_RY
+    assert np.max(np.abs(got.eigenvalues - g["eig_tol12"])) < FP64_EIG_TOL_RY
+    mixed = _solve(ap, rk.psi0, sy.nbands, 1e-10, 300, MIXED)
+    assert mixed.unconverged == 0
+    assert np.max(np.abs(mixed.eigenvalues - g["eig_tol12"])) < MIXED_EIG_TOL_RY
+
+
+# ------------------------------------------------ config 2: all 32 k-points
+
+def test_config2_all_kpoints(cuda_device):
+    g = _need(2)
+    sy = RF.system(2)
+    ap = _applicator()
+    nk = len(sy.kpoints)
+    assert nk == g["eig_tol10"].shape[0] == 32
+    for k in range(nk):
+        rk = RF.kpoint(sy, g, k)
+        RF.prepare_on_device(ap, sy, g, rk, k)
+        got = _solve(ap, rk.psi0, sy.nbands, 1e-10, 300)
+        assert got.unconverged == int(g["unconverged_tol10"][k]) == 0, k
+        assert abs(got.iterations - int(g["iterations_tol10"][k])) <= 1, k
+        assert np.max(np.abs(got.eigenvalues - g["eig_tol10"][k])) < FP64_EIG_TOL_RY, k
+        mixed = _solve(ap, rk.psi0, sy.nbands, 1e-10, 300, MIXED)
+        assert mixed.unconverged == 0, k
+        assert np.max(np.abs(mixed.eigenvalues - g["eig_tol10"][k])) < MIXED_EIG_TOL_RY, k
