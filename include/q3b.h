@@ -282,6 +282,17 @@ int q3b_hegv(q3b_context* ctx, int n, const q3b_cplx128* h_dev, const q3b_cplx12
  * replayed after that.  No counterpart in the reference (diagnostics). */
 int q3b_graph_stats(q3b_context* ctx, int* captures, int* replays);
 
+/* The plane-pass kernel of the local term for the prepared k-point, by
+ * precision (Q3B_FP64 or Q3B_MIXED's FP32 product).  choice: 0 hands it back
+ * to the autotuner (the default: the candidates are timed once per grid and
+ * precision); 128, 256 or 512 selects the shared-memory kernel with that many
+ * threads a plane; -1 or -2 the register kernel with one or two lanes a line,
+ * which exists for some grids only (Q3B_ERR_INVALID when not for this one).
+ * q3b_get_local_kernel reports the choice in force, tuning first if needed.
+ * No counterpart in the reference (its FFT is a library call). */
+int q3b_set_local_kernel(q3b_context* ctx, int precision, int choice);
+int q3b_get_local_kernel(q3b_context* ctx, int precision, int* choice);
+
 /* ---- projector set built on the device (ProjectorSetBuilder) ---------------- */
 
 /* q3b_prepare_kpoint with the Kleinman-Bylander projector matrix built on the

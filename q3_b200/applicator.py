@@ -248,6 +248,17 @@ class PlanewaveHamiltonianApplicator:
         self.npw = npw
         self.kpoint_index = kpoint_index
 
+    def set_local_kernel(self, choice: int, precision: int = FP64) -> None:
+        """Override the autotuner's plane kernel for the prepared k-point (q3b_set_local_kernel):
+        0 re-tunes, 128/256/512 the shared-memory kernel, -1/-2 the register kernel."""
+        check(self.h, self.lib.q3b_set_local_kernel(self.h, int(precision), int(choice)))
+
+    def local_kernel(self, precision: int = FP64) -> int:
+        """The plane kernel in force for the prepared k-point (tuning first if needed)."""
+        out = C.c_int()
+        check(self.h, self.lib.q3b_get_local_kernel(self.h, int(precision), C.byref(out)))
+        return out.value
+
     def projectors(self):
         """The prepared k-point's projector matrix as a CUDA tensor (P x npw)."""
         import ctypes as C

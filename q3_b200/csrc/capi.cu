@@ -202,6 +202,25 @@ int q3b_graph_stats(q3b_context* ctx, int* captures, int* replays) {
     return Q3B_OK;
 }
 
+int q3b_set_local_kernel(q3b_context* ctx, int precision, int choice) {
+    return guarded(ctx, [&](Context& c) {
+        c.require_ready();
+        if (precision == Q3B_FP64) c.set_local_kernel<double>(choice);
+        else if (precision == Q3B_MIXED) c.set_local_kernel<float>(choice);
+        else throw q3b::Status(Q3B_ERR_INVALID, "unknown precision");
+    });
+}
+
+int q3b_get_local_kernel(q3b_context* ctx, int precision, int* choice) {
+    return guarded(ctx, [&](Context& c) {
+        c.require_ready();
+        if (!choice) throw q3b::Status(Q3B_ERR_INVALID, "null output");
+        if (precision == Q3B_FP64) *choice = c.local_kernel<double>();
+        else if (precision == Q3B_MIXED) *choice = c.local_kernel<float>();
+        else throw q3b::Status(Q3B_ERR_INVALID, "unknown precision");
+    });
+}
+
 int q3b_accumulate_density(q3b_context* ctx, const q3b_cplx128* psi, int nvec, const double* weights,
                            double* rho) {
     return guarded(ctx, [&](Context& c) {

@@ -121,6 +121,9 @@ Context::Context(int dev, size_t hbm_budget) : device(dev), budget(hbm_budget) {
     Q3B_CUDA(cudaSetDevice(dev));
     Q3B_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
     stream = own_stream;
+    err_word.reserve(this, 4 * sizeof(int));
+    Q3B_CUDA(cudaMemsetAsync(err_word.ptr, 0, 4 * sizeof(int), stream));
+    Q3B_CUDA(cudaStreamSynchronize(stream));
 }
 
 Context::~Context() {
@@ -200,8 +203,8 @@ void Context::set_potential(const double* v, int a, int b, int c) {
     n3 = c;
     const size_t N = (size_t)a * b * c;
     v_host.assign(v, v + N);
-    std::vector<double> vp(N);
-    std::vector<float> vp32(N);
+    std::vector<double> vp(N), vn(N);
+    std::vector<float> vp32(N), vn32(N);
     const double inv = 1.0 / static_cast<double>(N);
     const std::vector<int> pos2 = transformed_positions(b), pos3 = transformed_positions(c);
     for (int w1 = 0; w1 < a; ++w1)
@@ -211,9 +214,14 @@ void Context::set_potential(const double* v, int a, int b, int c) {
                 const size_t d = ((size_t)pos3[w3] * a + w1) * b + pos2[w2];
                 vp[d] = s;
                 vp32[d] = static_cast<float>(s);
+                const size_t dn = ((size_t)pos3[w3] * a + w1) * b + w2;
+                vn[dn] = s;
+                vn32[dn] = static_cast<float>(s);
             }
     upload(this, v64, vp.data(), N);
     upload(this, v32, vp32.data(), N);
+    upload(this, v64nat, vn.data(), N);
+    upload(this, v32nat, vn32.data(), N);
     Q3B_CUDA(cudaStreamSynchronize(stream));
     pot_valid = true;
     if (regrid && kp.valid) {
@@ -226,6 +234,8 @@ void Context::set_potential(const double* v, int a, int b, int c) {
     }
     kp.lp64.vplane = v64.as<double>();
     kp.lp32.vplane = v32.as<float>();
+    kp.lp64.vnat = v64nat.as<double>();
+    kp.lp32.vnat = v32nat.as<float>();
 }
 
 template <typename T, typename R> static std::vector<T> twiddles(int n) {
@@ -236,6 +246,49 @@ template <typename T, typename R> static std::vector<T> twiddles(int n) {
         t[m].y = static_cast<R>(sinl(ang));
     }
     return t;
+}
+
+// The shape the register plane kernel needs (hpsi_local.cuh, LocalPlan::row_iv):
+// the rows w1 holding sticks form one cyclic interval starting at row_lo, and
+// in each of them the sticks' w2 form one cyclic interval.  On success `order`
+// lists the stick columns (w1*n2 + w2) row by row along those intervals and
+// ivs[s] = {first w2, count, first stick, 0} for row slot s.
+static bool cyclic_interval(const std::vector<char>& in, int n, int& lo, int& len) {
+    len = 0;
+    for (char c : in) len += c ? 1 : 0;
+    if (len == 0) return false;
+    if (len == n) {
+        lo = 0;
+        return true;
+    }
+    int starts = 0;
+    for (int i = 0; i < n; ++i)
+        if (in[i] && !in[(i + n - 1) % n]) {
+            lo = i;
+            ++starts;
+        }
+    return starts == 1;
+}
+
+static bool stick_intervals(const std::vector<int>& col_id, int n1, int n2, int& row_lo, std::vector<int4>& ivs,
+                            std::vector<int>& order) {
+    std::vector<char> has_row(n1, 0);
+    for (int col = 0; col < n1 * n2; ++col)
+        if (col_id[col] >= 0) has_row[col / n2] = 1;
+    int nrows = 0;
+    if (!cyclic_interval(has_row, n1, row_lo, nrows)) return false;
+    ivs.clear();
+    order.clear();
+    std::vector<char> in(n2);
+    for (int s = 0; s < nrows; ++s) {
+        const int w1 = (row_lo + s) % n1;
+        for (int w2 = 0; w2 < n2; ++w2) in[w2] = col_id[w1 * n2 + w2] >= 0;
+        int lo = 0, len = 0;
+        if (!cyclic_interval(in, n2, lo, len)) return false;
+        ivs.push_back(make_int4(lo, len, static_cast<int>(order.size()), 0));
+        for (int o = 0; o < len; ++o) order.push_back(w1 * n2 + (lo + o) % n2);
+    }
+    return true;
 }
 
 void Context::build_plan() {
@@ -261,19 +314,29 @@ void Context::build_plan() {
         gcol[g] = w1 * n2 + w2;
         col_id[gcol[g]] = 0;
     }
-    int S = 0;
-    std::vector<int> stick_pos, rows;
-    int last_row = -1;
-    for (int col = 0; col < n1 * n2; ++col) {
-        if (col_id[col] < 0) continue;
-        col_id[col] = S++;
-        const int w1 = col / n2, w2 = col % n2;
-        stick_pos.push_back(w1 * p2 + w2);
-        if (w1 != last_row) {
-            rows.push_back(w1 * p2);
-            last_row = w1;
-        }
+    // the columns in stick order: along the row intervals of the register
+    // plane kernel when the sticks have that shape, else row-major
+    int row_lo = 0;
+    std::vector<int4> ivs;
+    std::vector<int> order;
+    const bool intervals = stick_intervals(col_id, n1, n2, row_lo, ivs, order);
+    if (!intervals) {
+        order.clear();
+        for (int col = 0; col < n1 * n2; ++col)
+            if (col_id[col] >= 0) order.push_back(col);
     }
+    const int S = static_cast<int>(order.size());
+    std::vector<int> stick_pos(S), rows;
+    for (int i = 0; i < S; ++i) {
+        col_id[order[i]] = i;
+        stick_pos[i] = (order[i] / n2) * p2 + order[i] % n2;
+    }
+    for (int w1 = 0; w1 < n1; ++w1)
+        for (int w2 = 0; w2 < n2; ++w2)
+            if (col_id[w1 * n2 + w2] >= 0) {
+                rows.push_back(w1 * p2);
+                break;
+            }
     std::vector<int> start(S + 1, 0);
     for (int g = 0; g < k.npw; ++g)
         if (gcol[g] >= 0) start[col_id[gcol[g]] + 1]++;
@@ -295,6 +358,8 @@ void Context::build_plan() {
     upload(this, k.stick_pos, stick_pos.data(), stick_pos.size());
     upload(this, k.row_base, rows.data(), rows.size());
     upload(this, k.unmapped, unm.data(), unm.size());
+    if (intervals) upload(this, k.row_iv, ivs.data(), ivs.size());
+    else k.row_iv.release();
     const int dims[3] = {n1, n2, n3};
     for (int d = 0; d < 3; ++d) {
         auto t64 = twiddles<double2, double>(dims[d]);
@@ -338,9 +403,16 @@ void Context::build_plan() {
         lp.tw3 = tw[2].as<TT>();
         lp.ke = ke.as<std::remove_const_t<RR>>();
         lp.vplane = vv.as<std::remove_const_t<RR>>();
+        lp.xpitch = (S + 1) & ~1;
+        lp.row_lo = row_lo;
+        lp.row_iv = intervals ? k.row_iv.as<int4>() : nullptr;
+        lp.variant = 0;
+        lp.err = err_word.as<int>();
     };
     fillp(k.lp64, k.tw64, k.ke64, v64);
     fillp(k.lp32, k.tw32, k.ke32, v32);
+    k.lp64.vnat = v64nat.as<double>();
+    k.lp32.vnat = v32nat.as<float>();
     k.tuned64 = k.tuned32 = false;
     if (plane_smem_bytes(k.lp64) > 227 * 1024) {
         throw Status(Q3B_ERR_INVALID, "FFT plane " + std::to_string(n1) + "x" + std::to_string(n2) +
@@ -465,13 +537,24 @@ template <typename R> int Context::sticks_chunk(int nvec) const {
     return static_cast<int>(c);
 }
 
-// Tuning results by (grid, precision), shared by every context of the process:
-// the best block size of the plane kernel depends on the plane's shared-memory
-// footprint and line factors, so a new k-point or request on a grid seen
-// before reuses it instead of timing again.
+// Tuning results by (grid, precision, whether the register kernel applies),
+// shared by every context of the process: the best plane kernel depends on the
+// plane's shared-memory footprint and line factors, so a new k-point or request
+// on a grid seen before reuses it instead of timing again.  A choice is the
+// shared-memory kernel's block size (> 0) or minus the register kernel's lanes
+// a line (< 0).
 namespace {
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int>, int> g_tuned;
+std::map<std::tuple<int, int, int, int, int>, int> g_tuned;
+
+template <typename R> void set_choice(LocalPlan<R>& lp, int choice) {
+    if (choice > 0) {
+        lp.variant = 0;
+        lp.plane_threads = choice;
+    } else {
+        lp.variant = -choice;
+    }
+}
 }  // namespace
 
 template <typename R> void Context::tune_local() {
@@ -481,12 +564,12 @@ template <typename R> void Context::tune_local() {
     done = true;
     LocalPlan<R>& lp = const_cast<LocalPlan<R>&>(local_plan<R>());
     if (lp.nsticks == 0) return;
-    const auto key = std::make_tuple(lp.n1, lp.n2, lp.n3, (int)sizeof(R));
+    const auto key = std::make_tuple(lp.n1, lp.n2, lp.n3, (int)sizeof(R), lp.row_iv ? 1 : 0);
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tuned.find(key);
         if (it != g_tuned.end()) {
-            lp.plane_threads = it->second;
+            set_choice(lp, it->second);
             return;
         }
     }
@@ -499,14 +582,18 @@ template <typename R> void Context::tune_local() {
     Q3B_CUDA(cudaMemsetAsync(tin, 0, n * sizeof(T), stream));
     const int chunk = sticks_chunk<R>(nb);
     ws_sticks.reserve(this, (size_t)chunk * sticks_bytes_per_band(lp));
-    const int cand[3] = {128, 256, 512};
+    std::vector<int> cand = {128, 256, 512};
+    if (lp.row_iv) {
+        for (int lanes : {1, 2})
+            if (has_planes_reg(lp.n1, lp.n2, lanes)) cand.push_back(-lanes);
+    }
     cudaEvent_t e0, e1;
     Q3B_CUDA(cudaEventCreate(&e0));
     Q3B_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
-    int best_threads = lp.plane_threads;
-    for (int c = 0; c < 3; ++c) {
-        lp.plane_threads = cand[c];
+    int best_choice = lp.plane_threads;
+    for (size_t c = 0; c < cand.size(); ++c) {
+        set_choice(lp, cand[c]);
         float t = 1e30f;
         for (int rep = 0; rep < 3; ++rep) {
             Q3B_CUDA(cudaEventRecord(e0, stream));
@@ -519,18 +606,45 @@ template <typename R> void Context::tune_local() {
         }
         if (t < best) {
             best = t;
-            best_threads = cand[c];
+            best_choice = cand[c];
         }
     }
-    lp.plane_threads = best_threads;
+    set_choice(lp, best_choice);
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        g_tuned[key] = best_threads;
+        g_tuned[key] = best_choice;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     ws_tune.release();
 }
+
+template <typename R> void Context::set_local_kernel(int choice) {
+    LocalPlan<R>& lp = const_cast<LocalPlan<R>&>(local_plan<R>());
+    bool& tuned = std::is_same<R, double>::value ? kp.tuned64 : kp.tuned32;
+    if (choice == 0) {
+        tuned = false;
+        return;
+    }
+    if (choice > 0 && choice != 128 && choice != 256 && choice != 512)
+        throw Status(Q3B_ERR_INVALID, "plane kernel threads must be 128, 256 or 512");
+    if (choice < 0 && (!lp.row_iv || !has_planes_reg(lp.n1, lp.n2, -choice)))
+        throw Status(Q3B_ERR_INVALID, "no register plane kernel with " + std::to_string(-choice) +
+                                          " lanes a line for this grid and k-point");
+    set_choice(lp, choice);
+    tuned = true;
+}
+
+template <typename R> int Context::local_kernel() {
+    tune_local<R>();
+    const LocalPlan<R>& lp = local_plan<R>();
+    return lp.variant > 0 ? -lp.variant : lp.plane_threads;
+}
+
+template void Context::set_local_kernel<double>(int);
+template void Context::set_local_kernel<float>(int);
+template int Context::local_kernel<double>();
+template int Context::local_kernel<float>();
 
 template <typename R>
 void Context::apply_h(const cplx_t<R>* psi, long ldpsi, cplx_t<R>* hpsi, long ldh, int nvec,

@@ -54,6 +54,7 @@ struct KPoint {
     DevBuf qpk64, qpk32;
     // sticks plan
     DevBuf stick_start, entry_g, entry_w3, entry_stick, stick_pos, row_base, unmapped;
+    DevBuf row_iv;  // int4 per stick row (LocalPlan::row_iv), when the sticks allow it
     DevBuf tw64[3], tw32[3];
     LocalPlan<double> lp64{};
     LocalPlan<float> lp32{};
@@ -73,6 +74,8 @@ class Context {
     bool pot_valid = false;
     std::vector<double> v_host;     // V(r) as given, reference layout
     DevBuf v64, v32;                // V/N, [w3 pos][w1][w2 pos] (see LocalPlan::vplane)
+    DevBuf v64nat, v32nat;          // V/N, [w3 pos][w1][w2] (LocalPlan::vnat)
+    DevBuf err_word;                // device error word of this context's kernels (bounded waits)
 
     KPoint kp;
 
@@ -125,6 +128,9 @@ class Context {
     // Autotuner: time the candidate plane kernels on a few bands of this
     // k-point and keep the fastest (once per plan and precision).
     template <typename R> void tune_local();
+    // override of the tuner's plane kernel (q3b_set_local_kernel) and the choice in force
+    template <typename R> void set_local_kernel(int choice);
+    template <typename R> int local_kernel();
 
   private:
     void build_plan();

@@ -90,11 +90,79 @@ template <> struct Split<12> { static constexpr int A = 4, B = 3; };
 template <> struct Split<15> { static constexpr int A = 5, B = 3; };
 template <> struct Split<16> { static constexpr int A = 4, B = 4; };
 
+// Larger composites, for the register-resident line transforms of the plane
+// kernel (planes_reg.cu): a line of up to 108 points held by one to four lanes.
+template <> struct Split<18> { static constexpr int A = 6, B = 3; };
+template <> struct Split<20> { static constexpr int A = 5, B = 4; };
+template <> struct Split<24> { static constexpr int A = 8, B = 3; };
+template <> struct Split<25> { static constexpr int A = 5, B = 5; };
+template <> struct Split<27> { static constexpr int A = 9, B = 3; };
+template <> struct Split<30> { static constexpr int A = 10, B = 3; };
+template <> struct Split<32> { static constexpr int A = 8, B = 4; };
+template <> struct Split<36> { static constexpr int A = 9, B = 4; };
+template <> struct Split<40> { static constexpr int A = 8, B = 5; };
+template <> struct Split<45> { static constexpr int A = 9, B = 5; };
+template <> struct Split<48> { static constexpr int A = 16, B = 3; };
+template <> struct Split<50> { static constexpr int A = 10, B = 5; };
+template <> struct Split<54> { static constexpr int A = 9, B = 6; };
+template <> struct Split<60> { static constexpr int A = 15, B = 4; };
+template <> struct Split<64> { static constexpr int A = 16, B = 4; };
+template <> struct Split<72> { static constexpr int A = 9, B = 8; };
+template <> struct Split<80> { static constexpr int A = 16, B = 5; };
+template <> struct Split<108> { static constexpr int A = 12, B = 9; };
+
+// cos and sin of 2 pi m / N, m < N, as a table built at compile time: the
+// angle is reduced to a quadrant exactly in integers, and cos/sin of the
+// remainder (below pi/2) are summed from their Taylor series in double (27
+// terms; the first omitted term is below 1e-24).  Indexed with the constants
+// of unrolled loops, the table folds into literal operands.
+struct UnitTerms {
+    static constexpr double kHalfPi = 1.57079632679489661923;
+    static constexpr double cos_q(double x) {
+        double term = 1.0, sum = 1.0;
+        for (int k = 1; k < 14; ++k) {
+            term *= -x * x / ((2.0 * k - 1.0) * (2.0 * k));
+            sum += term;
+        }
+        return sum;
+    }
+    static constexpr double sin_q(double x) {
+        double term = x, sum = x;
+        for (int k = 1; k < 14; ++k) {
+            term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
+            sum += term;
+        }
+        return sum;
+    }
+};
+
+template <int N> struct UnitTable {
+    double c[N];
+    double s[N];
+    constexpr UnitTable() : c(), s() {
+        for (int m = 0; m < N; ++m) {
+            const int q = (4 * m) / N;             // quadrant
+            const int r = 4 * m - q * N;           // remainder, in units of (pi/2)/N
+            const double x = UnitTerms::kHalfPi * static_cast<double>(r) / static_cast<double>(N);
+            const double cx = r == 0 ? 1.0 : UnitTerms::cos_q(x);
+            const double sx = r == 0 ? 0.0 : UnitTerms::sin_q(x);
+            c[m] = q == 0 ? cx : q == 1 ? -sx : q == 2 ? -cx : sx;
+            s[m] = q == 0 ? sx : q == 1 ? cx : q == 2 ? -sx : -cx;
+        }
+    }
+};
+
 // cos(2 pi m / N) and sin(2 pi m / N) for m < N, the internal twiddles of the
 // composite small DFTs (plain trigonometry, evaluated in extended precision and
-// rounded to double)
-template <int N> __host__ __device__ constexpr double unit_cos(int m);
-template <int N> __host__ __device__ constexpr double unit_sin(int m);
+// rounded to double; the sizes without a literal table below use UnitTable)
+template <int N> __host__ __device__ constexpr double unit_cos(int m) {
+    constexpr UnitTable<N> t{};
+    return t.c[m];
+}
+template <int N> __host__ __device__ constexpr double unit_sin(int m) {
+    constexpr UnitTable<N> t{};
+    return t.s[m];
+}
 template <> __host__ __device__ constexpr double unit_cos<6>(int m) {
     constexpr double t[6] = {1.0, 0.5, -0.5, -1.0, -0.5, 0.5};
     return t[m];

@@ -96,10 +96,10 @@ sticks_backward(LocalPlan<R> p, const cplx_t<R>* __restrict__ psi, long ldpsi, c
     __syncthreads();
     fft::LineGeom g{p.n3, p.na3, p.nb3, ns, p.p3, 1, nullptr};
     fft::backward<MAXR>(lines, g, tw);
-    T* xb = X + (long)band * p.n3 * p.nsticks;
+    T* xb = X + (long)band * p.n3 * p.xpitch;
     for (int idx = threadIdx.x; idx < ns * p.n3; idx += blockDim.x) {
         const int s = idx % ns, i3 = idx / ns;
-        xb[(long)i3 * p.nsticks + s0 + s] = lines[s * p.p3 + i3];
+        xb[(long)i3 * p.xpitch + s0 + s] = lines[s * p.p3 + i3];
     }
 }
 
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(NT, (plane_min_blocks<R, NT, MAXR>())) planes(
     // column transform reads the others as zero, and writes back only these
     zero_stick_rows(p, rowb, plane);
     __syncthreads();
-    T* xp = X + ((long)band * p.n3 + i3) * p.nsticks;
+    T* xp = X + ((long)band * p.n3 + i3) * p.xpitch;
     for (int s = threadIdx.x; s < p.nsticks; s += NT) plane[p.stick_pos[s]] = xp[s];
     __syncthreads();
     fft::LineGeom gr{p.n2, p.na2, p.nb2, p.nrows, 0, 1, rowb};
@@ -155,14 +155,14 @@ sticks_forward(LocalPlan<R> p, const cplx_t<R>* __restrict__ X, const cplx_t<R>*
     const int s0 = blockIdx.x * p.sg;
     const int ns = min(p.sg, p.nsticks - s0);
     for (int i = threadIdx.x; i < p.n3; i += blockDim.x) tw[i] = p.tw3[i];
-    const T* xb = X + (long)band * p.n3 * p.nsticks;
+    const T* xb = X + (long)band * p.n3 * p.xpitch;
     const int total = ns * p.n3;
     for (int ib = threadIdx.x; ib < total; ib += kLoadBatch * blockDim.x) {
         T v[kLoadBatch];
 #pragma unroll
         for (int u = 0; u < kLoadBatch; ++u) {
             const int idx = ib + u * blockDim.x;
-            if (idx < total) v[u] = xb[(long)(idx / ns) * p.nsticks + s0 + idx % ns];
+            if (idx < total) v[u] = xb[(long)(idx / ns) * p.xpitch + s0 + idx % ns];
         }
 #pragma unroll
         for (int u = 0; u < kLoadBatch; ++u) {
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(256, 2) planes_density(LocalPlan<double> p, co
         if (wb == 0.0) continue;
         zero_stick_rows(p, rowb, plane);
         __syncthreads();
-        const T* xp = X + ((long)b * p.n3 + i3) * p.nsticks;
+        const T* xp = X + ((long)b * p.n3 + i3) * p.xpitch;
         for (int s = threadIdx.x; s < p.nsticks; s += blockDim.x) plane[p.stick_pos[s]] = xp[s];
         __syncthreads();
         fft::backward<MAXR>(plane, gr, tw2);
@@ -391,7 +391,9 @@ void apply_local(cudaStream_t st, const LocalPlan<R>& p, const cplx_t<R>* psi, l
             if (tm) tm->begin(PhaseTimer::PLANES);
             const dim3 gp(p.n3, nb);
             const bool small12 = p.na1 <= kSmallR && p.nb1 <= kSmallR && p.na2 <= kSmallR && p.nb2 <= kSmallR;
-            if (small12) {
+            if (p.variant > 0 && launch_planes_reg<R>(p, X, nb, p.variant, st, p.err)) {
+                // the register kernel took the plane pass
+            } else if (small12) {
                 if (p.plane_threads >= 512) launch_planes<R, 512, kSmallR>(gp, smem_p, st, p, X);
                 else if (p.plane_threads >= 256) launch_planes<R, 256, kSmallR>(gp, smem_p, st, p, X);
                 else launch_planes<R, 128, kSmallR>(gp, smem_p, st, p, X);

@@ -41,11 +41,31 @@ template <typename R> struct LocalPlan {
     const R* ke;             // |k+G|^2 (Ry), caller's order
     const R* vplane;         // V(r)/N laid out [w3 pos][w1][w2 pos], with the w3 and w2
                              // positions of the backward transform's digit-reversed order
+    // stick buffer X[band][w3 pos][stick]: sticks of one (band, w3) plane are
+    // xpitch apart (nsticks rounded up to an even count, so every plane's run
+    // starts on a 16-byte boundary for the bulk copies of planes_reg.cu)
+    int xpitch;
+    // Register plane kernel (planes_reg.cu): the stick rows are the cyclic
+    // interval row_lo .. row_lo + nrows - 1 of w1, row slot s holding
+    // row_iv[s] = {first w2, count, first stick, 0} (its sticks a cyclic
+    // interval of w2, numbered consecutively).  row_iv is null when the
+    // k-point's sticks do not have that shape.
+    int row_lo;
+    const int4* row_iv;
+    const R* vnat;           // V(r)/N laid out [w3 pos][w1][w2], w1 and w2 natural
+    int variant;             // plane kernel: 0 shared-memory (plane_threads), L > 0 register with L lanes a line
+    int* err;                // the context's device error word (bounded waits that ran out)
 };
+
+// the register plane kernel: whether there is one for an n1 x n2 plane with
+// `lanes` lanes a line, and its launch (false when the plan or grid has none)
+bool has_planes_reg(int n1, int n2, int lanes);
+template <typename R>
+bool launch_planes_reg(const LocalPlan<R>& p, cplx_t<R>* X, int nb, int lanes, cudaStream_t st, int* err);
 
 // bytes of the stick buffer per band
 template <typename R> inline size_t sticks_bytes_per_band(const LocalPlan<R>& p) {
-    return (size_t)p.n3 * p.nsticks * sizeof(cplx_t<R>);
+    return (size_t)p.n3 * p.xpitch * sizeof(cplx_t<R>);
 }
 
 // Per-kernel-class CUDA-event timing of one application (diagnostics).
