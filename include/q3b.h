@@ -157,6 +157,12 @@ typedef struct {
 int q3b_apply_h_timed(q3b_context* ctx, const void* psi_dev, void* hpsi_dev, int nvec, int fp32,
                       q3b_apply_timing* timing);
 
+/* The FP64 FMA throughput of the context's GPU in TFLOP/s, measured by a
+ * probe kernel of independent DFMA chains (a few milliseconds): the
+ * denominator of the FP64 GEMMs' roofline.  No counterpart in the reference
+ * (diagnostics). */
+int q3b_measure_fp64_rate(q3b_context* ctx, double* tflops);
+
 /* Kernel launches the library has issued in this process (all contexts). */
 unsigned long long q3b_kernel_launches(void);
 

@@ -110,6 +110,7 @@ SIGNATURES = {
     "q3b_accumulate_density": (_i, [_vp, _vp, _i, _vp, _vp]),
     "q3b_graph_stats": (_i, [_vp, C.POINTER(_i), C.POINTER(_i)]),
     "q3b_set_local_kernel": (_i, [_vp, _i, _i]),
+    "q3b_measure_fp64_rate": (_i, [_vp, C.POINTER(C.c_double)]),
     "q3b_get_local_kernel": (_i, [_vp, _i, C.POINTER(_i)]),
     "q3b_prepare_kpoint_build": (_i, [_vp, _i, _vp, _vp, _vp, C.c_double, _i, _vp, _vp, _i, _vp, _vp, _i,
                                       C.c_double, _vp, _vp]),

@@ -272,6 +272,13 @@ int q3b_apply_h_timed(q3b_context* ctx, const void* psi, void* hpsi, int nvec, i
 
 unsigned long long q3b_kernel_launches(void) { return q3b::launches(); }
 
+int q3b_measure_fp64_rate(q3b_context* ctx, double* tflops) {
+    return guarded(ctx, [&](Context& c) {
+        if (!tflops) throw q3b::Status(Q3B_ERR_INVALID, "null output");
+        *tflops = q3b::measure_dfma_tflops(c.stream);
+    });
+}
+
 int q3b_gemm(q3b_context* ctx, char ta, char tb, int m, int n, int k, q3b_cplx128 alpha, const q3b_cplx128* a,
              int lda, const q3b_cplx128* b, int ldb, q3b_cplx128 beta, q3b_cplx128* cc, int ldc) {
     return guarded(ctx, [&](Context& c) { gemm_entry<double>(c, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, cc, ldc); });

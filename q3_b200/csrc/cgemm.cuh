@@ -25,6 +25,10 @@ void cgemm(cudaStream_t st, bool conj_a, int M, int N, int K, cplx_t<R> alpha, c
            long lda, const cplx_t<R>* B, long ldb, cplx_t<R> beta, cplx_t<R>* C, long ldc,
            const GemmWorkspace& ws);
 
+// DFMA throughput of the current device (TFLOP/s), from a probe kernel of
+// independent FMA chains (the FP64 roofline's denominator)
+double measure_dfma_tflops(cudaStream_t st);
+
 // bytes of workspace cgemm may use for a C,N product of this shape
 template <typename R> size_t cgemm_workspace_bytes(int M, int N, int K);
 
