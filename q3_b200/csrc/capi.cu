@@ -15,6 +15,7 @@ template <typename F> int guarded(q3b_context* c, F&& f) {
     if (!c) return Q3B_ERR_INVALID;
     try {
         Q3B_CUDA(cudaSetDevice(c->impl.device));
+        q3b::tc::ErrorScope scope(c->impl.err_word.as<int>());
         f(c->impl);
         return Q3B_OK;
     } catch (const std::exception& e) {

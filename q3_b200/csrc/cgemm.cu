@@ -325,13 +325,12 @@ __global__ void splitk_reduce(int M, int N, int splits, const cplx_t<R>* __restr
 // Products whose 64x64 tiling has fewer tiles than the GPU has SMs (the
 // subspace eigensolver's n x n x n products up to n = 767) run on 32x32 tiles:
 // four times the blocks and a quarter of the serial K loop per block.
-constexpr long kSmallTiles = 148;
-inline bool small_tiles(int M, int N) { return (long)ceil_div(M, kBM) * ceil_div(N, kBN) < kSmallTiles; }
+inline bool small_tiles(int M, int N) { return (long)ceil_div(M, kBM) * ceil_div(N, kBN) < device_sms(); }
 
 // K splits for a product with `tiles` output tiles (never more than for
 // 64x64 tiles, which size the workspace)
 inline int choose_splits_for(int tiles, int K) {
-    const int target = 2 * 148;
+    const int target = 2 * device_sms();
     int s = ceil_div(target, tiles);
     const int kmax = ceil_div(K, 128);
     if (s > kmax) s = kmax;
@@ -376,9 +375,7 @@ void zgemm_big_run(cudaStream_t st, dim3 grid, int M, int N, int K, double2 alph
 void zgemm_big_launch(cudaStream_t st, bool conj_a, int M, int N, int K, double2 alpha, const double2* A,
                       long lda, const double2* B, long ldb, double2 beta, double2* C, long ldc,
                       const GemmWorkspace& ws) {
-    int dev = 0, sms = 148;
-    Q3B_CUDA(cudaGetDevice(&dev));
-    Q3B_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int sms = device_sms();
     auto waves = [&](long units) { return (units + sms - 1) / sms; };
     const int t128 = ceil_div(M, 128) * ceil_div(N, big::BN), t96 = ceil_div(M, 96) * ceil_div(N, big::BN);
     int splits = 1, tm = 8, tiles = t128;

@@ -59,8 +59,20 @@ void pack_a(cudaStream_t st, int M, int K, const float2* A, long lda, bool kmajo
 void cgemm_packed(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, const PackedA& A,
                   const float2* B, long ldb, float2 beta, float2* C, long ldc, const GemmWorkspace& ws);
 size_t workspace_bytes(int M, int N, int K);
-// device word the tensor-core kernels set when a pipeline wait times out
+// device word the tensor-core kernels set when a pipeline wait times out: the
+// word of the context the calling thread works for (ErrorScope), so that
+// contexts used by different threads at once report only their own timeouts;
+// a process-wide word per device outside any context
 int* error_word();
+struct ErrorScope {
+    explicit ErrorScope(int* word);
+    ~ErrorScope();
+    ErrorScope(const ErrorScope&) = delete;
+    ErrorScope& operator=(const ErrorScope&) = delete;
+
+  private:
+    int* prev_;
+};
 // read (and clear) it; throws CudaError when it was set.  Synchronises st.
 void check_error(cudaStream_t st);
 }  // namespace tc

@@ -546,10 +546,10 @@ __global__ void splitk_sum(int M, int N, int splits, const float2* __restrict__ 
     }
 }
 
-// one block per SM: keep tiles x splits within one wave of 148
+// one block per SM: keep tiles x splits within one wave
 int choose_splits(int M, int N, int K) {
     const int tiles = ceil_div(M, BM) * ceil_div(N, BN);
-    int s = 148 / tiles;
+    int s = device_sms() / tiles;
     const int kmax = ceil_div(K, 256);
     if (s > kmax) s = kmax;
     if (s < 1) s = 1;
@@ -561,7 +561,15 @@ __device__ int g_tc_error;
 
 }  // namespace
 
+namespace {
+thread_local int* t_context_word = nullptr;
+}  // namespace
+
+ErrorScope::ErrorScope(int* word) : prev_(t_context_word) { t_context_word = word; }
+ErrorScope::~ErrorScope() { t_context_word = prev_; }
+
 int* error_word() {
+    if (t_context_word) return t_context_word;
     // per host thread: the device it last asked for and the word's address there
     thread_local int cached_dev = -1;
     thread_local int* cached = nullptr;
@@ -583,7 +591,7 @@ void check_error(cudaStream_t st) {
     Q3B_CUDA(cudaStreamSynchronize(st));
     if (hb[0]) {
         Q3B_CUDA(cudaMemsetAsync(w, 0, sizeof(int), st));
-        throw CudaError("tensor-core GEMM: a pipeline wait timed out");
+        throw CudaError("a bounded device wait timed out (tensor-core GEMM pipeline or plane-kernel stick copy)");
     }
 }
 
@@ -602,8 +610,8 @@ void launch(cudaStream_t st, bool conj_a, int M, int N, int K, float2 alpha, con
             const unsigned char* Apk, const float2* B, long ldb, float2 beta, float2* C, long ldc,
             const GemmWorkspace& ws) {
     int* err = error_word();
-    static std::once_flag once;
-    std::call_once(once, [] {
+    static PerDeviceOnce once;
+    once.run([] {
         set_kernel_smem<true, false>();
         set_kernel_smem<false, false>();
         set_kernel_smem<true, true>();
@@ -655,8 +663,8 @@ size_t packed_a_bytes(int M, int K) {
 
 void pack_a(cudaStream_t st, int M, int K, const float2* A, long lda, bool kmajor, unsigned char* out) {
     if (M <= 0 || K <= 0) return;
-    static std::once_flag once;
-    std::call_once(once, [] {
+    static PerDeviceOnce once;
+    once.run([] {
         cudaFuncSetAttribute(pack_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, A_TILE);
     });
     const int nkt = ceil_div(K, BK);

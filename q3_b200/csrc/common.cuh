@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -101,5 +102,35 @@ void* host_readback(size_t bytes);
 void upload_async(void* dst, const void* src, size_t bytes, cudaStream_t st);
 
 inline int ceil_div(long a, long b) { return static_cast<int>((a + b - 1) / b); }
+
+// Streaming multiprocessors of the current device (looked up once per device).
+int device_sms();
+
+// Grid of `threads`-thread blocks for a grid-stride loop over n items: one
+// block per `threads` items, at most `per_sm` blocks per SM of the device.
+inline int stride_grid(long n, int per_sm, int threads = 256) {
+    long b = (n + threads - 1) / threads;
+    const long cap = (long)device_sms() * per_sm;
+    if (b > cap) b = cap;
+    return static_cast<int>(b < 1 ? 1 : b);
+}
+
+// Runs a set-up step (function attributes, which belong to a function on one
+// device) the first time it is called with each device current.
+class PerDeviceOnce {
+  public:
+    template <typename F> void run(F&& f) {
+        int dev = 0;
+        Q3B_CUDA(cudaGetDevice(&dev));
+        std::lock_guard<std::mutex> lk(mu_);
+        if (dev >= 0 && dev < 64 && ((done_ >> dev) & 1ull)) return;
+        f();
+        if (dev >= 0 && dev < 64) done_ |= 1ull << dev;
+    }
+
+  private:
+    std::mutex mu_;
+    unsigned long long done_ = 0;
+};
 
 }  // namespace q3b

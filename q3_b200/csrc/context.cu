@@ -670,6 +670,21 @@ void Context::apply_h(const cplx_t<R>* psi, long ldpsi, cplx_t<R>* hpsi, long ld
 template void Context::apply_h<double>(const double2*, long, double2*, long, int, PhaseTimer*);
 template void Context::apply_h<float>(const float2*, long, float2*, long, int, PhaseTimer*);
 
+int device_sms() {
+    static std::atomic<int> cached[64] = {};
+    int dev = 0;
+    Q3B_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64) {
+        const int c = cached[dev].load(std::memory_order_relaxed);
+        if (c > 0) return c;
+    }
+    int sms = 0;
+    Q3B_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (sms < 1) sms = 1;
+    if (dev >= 0 && dev < 64) cached[dev].store(sms, std::memory_order_relaxed);
+    return sms;
+}
+
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 unsigned long long launches() { return g_launches.load(); }

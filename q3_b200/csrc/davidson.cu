@@ -38,11 +38,7 @@ constexpr double kEmptyFloor = 1e-5;        // tolerances.hpp:66
 constexpr double kStallBelow = 1e-5;        // Ry: the FP32 phase may stop on a plateau below this
 constexpr int kFlatIterations = 4;          // FP32 phase: iterations without a new band-energy low
 
-inline int grid_for(long n) {
-    long b = (n + 255) / 256;
-    if (b > 148L * 16) b = 148L * 16;
-    return static_cast<int>(b < 1 ? 1 : b);
-}
+inline int grid_for(long n) { return stride_grid(n, 16); }
 
 // R[:, j] /= max(0.5 (1 + x + sqrt(1 + (x-1)^2)), 1e-4), x = KE - eps_j
 // (subspace_manager/serial.hpp:1138-1156)

@@ -277,11 +277,7 @@ __global__ void copy_matrix(int n, const double2* src, int lds, double2* dst, in
     }
 }
 
-inline int grid_for(long n) {
-    long b = (n + 255) / 256;
-    if (b > 148L * 8) b = 148L * 8;
-    return static_cast<int>(b < 1 ? 1 : b);
-}
+inline int grid_for(long n) { return stride_grid(n, 8); }
 
 // ------------------------------------------------------------ grid barrier
 // One monotonic arrival counter: the e-th barrier of a launch completes when
@@ -927,7 +923,7 @@ size_t hegv_scratch_bytes(int n) {
     // eigenvector; a few length-n vectors; 256-byte alignment slack
     const size_t nn = (size_t)n * n;
     return potrf_scratch_bytes(n) + 5 * nn * sizeof(double2) + nn * (sizeof(double2) + 6 * sizeof(double)) +
-           nn * sizeof(double2) + 64 * (size_t)n * sizeof(double2) + 2 * 148 * sizeof(double2) +
+           nn * sizeof(double2) + 64 * (size_t)n * sizeof(double2) + 2 * (size_t)device_sms() * sizeof(double2) +
            (size_t)n * sizeof(unsigned) + 64 * 1024;
 }
 
@@ -988,8 +984,8 @@ HeevPlan heev_plan(int n, int nvec, Scratch& ws) {
     Q3B_CUDA(cudaGetDevice(&device));
     int nsm = 0;
     Q3B_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-    static std::once_flag once_inv;
-    std::call_once(once_inv, [] {
+    static PerDeviceOnce once_inv;
+    once_inv.run([] {
         cudaFuncSetAttribute(tridiag_invit_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvitSmemLimit);
     });
     // blocks: about 8 columns each, at most one per SM; columns (and W) in shared memory
@@ -1004,8 +1000,8 @@ HeevPlan heev_plan(int n, int nvec, Scratch& ws) {
     p.partial = ws.take<double2>(2 * (size_t)p.G);
     p.bar = ws.take<unsigned>(2);
     p.err = ws.take<int>(1);
-    static std::once_flag once;
-    std::call_once(once, [limit] {
+    static PerDeviceOnce once;
+    once.run([limit] {
         cudaFuncSetAttribute(hetrd_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit);
         cudaFuncSetAttribute(tridiag_invit_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvitSmemLimit);
     });

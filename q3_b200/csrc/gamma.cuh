@@ -76,10 +76,6 @@ __global__ void gamma_real_origin(int ncols, T* V, long ldv) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < ncols; j += gridDim.x * blockDim.x) V[(long)j * ldv].y = 0;
 }
 
-inline int gamma_blocks(long n) {
-    long b = (n + 255) / 256;
-    if (b > 148L * 16) b = 148L * 16;
-    return static_cast<int>(b < 1 ? 1 : b);
-}
+inline int gamma_blocks(long n) { return stride_grid(n, 16); }
 
 }  // namespace q3b

@@ -234,8 +234,8 @@ template <typename R, int MAXR> void set_limits_for() {
 }
 
 template <typename R> void set_smem_limits() {
-    static std::once_flag once;
-    std::call_once(once, [] {
+    static PerDeviceOnce once;
+    once.run([] {
         set_limits_for<R, kSmallR>();
         set_limits_for<R, 16>();
     });
@@ -433,8 +433,8 @@ bool density_small_factors(const LocalPlan<double>& p) {
 }
 
 void set_density_limits() {
-    static std::once_flag once;
-    std::call_once(once, [] {
+    static PerDeviceOnce once;
+    once.run([] {
         cudaFuncSetAttribute(planes_density<kSmallR>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         cudaFuncSetAttribute(planes_density<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     });

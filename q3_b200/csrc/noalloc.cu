@@ -55,6 +55,7 @@ extern "C" int q3b_apply_h_noalloc(q3b_context* ctx, const q3b_cplx128* psi, q3b
     q3b::Context& c = ctx->impl;
     try {
         Q3B_CUDA(cudaSetDevice(c.device));
+        q3b::tc::ErrorScope scope(c.err_word.as<int>());
         c.require_ready();
         if (nvec < 0 || (nvec > 0 && (!psi || !hpsi))) throw q3b::Status(Q3B_ERR_INVALID, "bad vectors");
         if (nvec == 0) return Q3B_OK;

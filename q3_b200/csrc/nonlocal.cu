@@ -43,12 +43,7 @@ __global__ void convert_kernel(long n, const cplx_t<RI>* __restrict__ in, cplx_t
     }
 }
 
-inline int grid_for(long n) {
-    long b = (n + 255) / 256;
-    if (b > 148L * 16) b = 148L * 16;
-    if (b < 1) b = 1;
-    return static_cast<int>(b);
-}
+inline int grid_for(long n) { return stride_grid(n, 16); }
 
 }  // namespace
 

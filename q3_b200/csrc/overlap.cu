@@ -22,11 +22,7 @@ __global__ void add_widened(long n, const double2* __restrict__ psi, const float
     }
 }
 
-inline int blocks_for(long n) {
-    long b = (n + 255) / 256;
-    if (b > 148L * 16) b = 148L * 16;
-    return static_cast<int>(b < 1 ? 1 : b);
-}
+inline int blocks_for(long n) { return stride_grid(n, 16); }
 
 }  // namespace
 
@@ -73,6 +69,7 @@ template <typename F> int overlap_guarded(q3b_context* c, F&& f) {
     if (!c) return Q3B_ERR_INVALID;
     try {
         Q3B_CUDA(cudaSetDevice(c->impl.device));
+        q3b::tc::ErrorScope scope(c->impl.err_word.as<int>());
         f(c->impl);
         return Q3B_OK;
     } catch (const std::exception& e) {

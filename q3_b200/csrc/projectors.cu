@@ -140,6 +140,7 @@ extern "C" int q3b_prepare_kpoint_build(q3b_context* ctx, int npw, const int32_t
     q3b::Context& c = ctx->impl;
     try {
         Q3B_CUDA(cudaSetDevice(c.device));
+        q3b::tc::ErrorScope scope(c.err_word.as<int>());
         if (npw <= 0 || !kpg_cart || !(cell_volume > 0.0) || natoms < 0 || nspecies < 0 || nq < 0 ||
             (natoms > 0 && (!positions || !species_of_atom || !d_blocks)) || (nspecies > 0 && !nbeta_of_species) ||
             (nq > 0 && !(dq > 0.0)))
@@ -216,6 +217,7 @@ extern "C" int q3b_get_projectors(q3b_context* ctx, q3b_cplx128* beta_dev, int* 
     q3b::Context& c = ctx->impl;
     try {
         Q3B_CUDA(cudaSetDevice(c.device));
+        q3b::tc::ErrorScope scope(c.err_word.as<int>());
         c.require_ready();
         if (nproj) *nproj = c.kp.nproj;
         if (beta_dev && c.kp.nproj > 0) {

@@ -166,6 +166,7 @@ class Server {
         Context& c = ctx->impl;
         try {
             Q3B_CUDA(cudaSetDevice(c.device));
+            q3b::tc::ErrorScope scope(c.err_word.as<int>());
             c.set_potential(j.v.data(), j.n1, j.n2, j.n3);
             c.prepare_kpoint(j.npw, j.g2g.data(), j.ke.data(), j.nproj ? j.beta.data() : nullptr, j.nproj,
                              j.natoms, j.nproj ? j.offs.data() : nullptr, j.nproj ? j.dblk.data() : nullptr);

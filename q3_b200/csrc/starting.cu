@@ -15,6 +15,7 @@ template <typename F> int guarded_start(q3b_context* ctx, F&& f) {
     if (!ctx) return Q3B_ERR_INVALID;
     try {
         Q3B_CUDA(cudaSetDevice(ctx->impl.device));
+        q3b::tc::ErrorScope scope(ctx->impl.err_word.as<int>());
         f(ctx->impl);
         return Q3B_OK;
     } catch (const std::exception& e) {
