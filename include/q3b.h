@@ -186,6 +186,11 @@ typedef struct {
                                     rows past the iterations run are left as they are.  The
                                     serving API ignores it.                                  */
     int history_rows;            /* rows of eigenvalue_history (0: no history)              */
+    int mixed_expansion_factor;  /* MIXED: basis expansion factor of the FP32 phase (no
+                                    counterpart in the reference; the FP64 refinement takes
+                                    basis_expansion_factor); 0 (the default) takes 4, else 3,
+                                    when that subspace order is within the eigensolver's
+                                    limit, else basis_expansion_factor                      */
 } q3b_davidson_opts;
 
 typedef struct {

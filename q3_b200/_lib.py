@@ -51,7 +51,8 @@ class DavidsonOpts(C.Structure):
                 ("basis_expansion_factor", C.c_int), ("occupied_bands", C.c_int),
                 ("precision", C.c_int), ("refine_sweeps", C.c_int),
                 ("mixed_tolerance", C.c_double), ("profile_stages", C.c_int),
-                ("eigenvalue_history", C.c_void_p), ("history_rows", C.c_int)]
+                ("eigenvalue_history", C.c_void_p), ("history_rows", C.c_int),
+                ("mixed_expansion_factor", C.c_int)]
 
 
 class DavidsonStats(C.Structure):

@@ -310,6 +310,7 @@ void q3b_davidson_default_opts(q3b_davidson_opts* o) {
     o->profile_stages = 0;
     o->eigenvalue_history = nullptr;
     o->history_rows = 0;
+    o->mixed_expansion_factor = 0;
 }
 
 int q3b_davidson_solve_dev(q3b_context* ctx, q3b_cplx128* bands, double* eig, int nb,

@@ -82,6 +82,7 @@ class Context {
     // workspaces
     DevBuf ws_sticks, ws_gemm, ws_bm, ws_bp, ws_conv_in, ws_conv_out, ws_host_io;
     DevBuf ws_solver, ws_dense, ws_bands, ws_tune;
+    DevBuf ws_mixed;  // FP64 bands of a mixed solve between its phases (buffer bands included)
     // replays of the dense eigensolver's launch sequence (one per context)
     dense::HegvGraphs hegv_graphs;
     // charge density: per-group partial sums and the band weights

@@ -753,6 +753,27 @@ template <typename R> class Davidson {
 
 }  // namespace
 
+int mixed_bands(int nb, int npw) { return std::min(npw, nb + std::max(2, (nb + 7) / 8)); }
+
+// The basis factor of the mixed solve's FP32 phase: a larger basis cuts that
+// phase's iterations (config 1: 94 -> 36 at factor 4), and with them its
+// subspace eigensolves, which both precisions pay once per iteration.  The
+// FP64 path and the mixed solve's FP64 refinement keep the reference's factor.
+int basis_factor(const q3b_davidson_opts& o, int nb, int npw) {
+    if (o.precision != Q3B_MIXED) return o.basis_expansion_factor;
+    int factor = o.mixed_expansion_factor;
+    if (factor <= 0) {
+        factor = o.basis_expansion_factor;
+        for (int f : {4, 3})
+            if (f > factor && dense::order_supported(std::min(f * mixed_bands(nb, npw), npw))) {
+                factor = f;
+                break;
+            }
+    }
+    if (factor < 2) throw Status(Q3B_ERR_INVALID, "mixed_expansion_factor must be >= 2");
+    return factor;
+}
+
 void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, const q3b_davidson_opts& o,
                     q3b_davidson_stats* stats) {
     c.require_ready();
@@ -769,6 +790,7 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         throw Status(Q3B_ERR_INVALID, "eigenvalue_history needs history_rows >= 0 and a buffer");
     std::vector<double> hist;
     std::vector<double>* rec = o.history_rows > 0 ? &hist : nullptr;
+    size_t hist_width = (size_t)nb;
     if (o.precision == Q3B_FP64) {
         Davidson<double> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
         dv.record_history(rec);
@@ -784,32 +806,45 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         Q3B_CUDA(cudaStreamSynchronize(c.stream));
         s.fp64_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     } else if (o.precision == Q3B_MIXED) {
+        const int factor = basis_factor(o, nb, npw);
+        // Both phases solve for nbi = nb + a few buffer bands, held to the loose
+        // tolerance of empty bands; the lowest nb are returned.  Without them the
+        // block's top band, whose gap to the first band outside the block is small,
+        // converges so slowly in the refinement that its eigenvalue change can drop
+        // below the tolerance while it is still 1e-8 to 1e-7 Ry from its limit.
+        const int nbi = mixed_bands(nb, npw);
+        c.ws_mixed.reserve(&c, (size_t)npw * nbi * sizeof(double2));
+        double2* mix = c.ws_mixed.as<double2>();
+        std::vector<double> stored_i(nbi, 0.0);
+        std::copy(stored.begin(), stored.end(), stored_i.begin());
         // FP32 phase to the loose tolerance
         std::vector<double> eig32;
         int it32 = 0, h32 = 0, col32 = 0;
         {
-            Davidson<float> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
+            Davidson<float> dv(c, nbi, factor, c.ws_solver, c.ws_dense);
             dv.record_history(rec);
             convert<double, float>(c.stream, (long)npw * nb, bands_dev, dv.V());
             const double tol32 = o.mixed_tolerance > 0.0 ? o.mixed_tolerance : 1e-6;
-            auto r = dv.solve(nb, stored, std::max(tol32, o.tolerance), std::max(1, o.max_iterations),
+            auto r = dv.solve(nb, stored_i, std::max(tol32, o.tolerance), std::max(1, o.max_iterations),
                               occupied, dv.scratch(), false, o.profile_stages ? s.stage_ms : nullptr, true);
-            // widen the FP32 Ritz vectors into the caller's bands
-            convert<float, double>(c.stream, (long)npw * nb, dv.scratch(), bands_dev);
+            // widen the FP32 Ritz vectors for the refinement
+            convert<float, double>(c.stream, (long)npw * nbi, dv.scratch(), mix);
             eig32 = r.eig;
             it32 = r.iterations;
             h32 = dv.happly();
             col32 = r.collapses;
         }
-        // FP64 refinement sweeps from the FP32 Ritz pairs
+        // FP64 refinement sweeps from the FP32 Ritz pairs, at the reference's factor
         const auto t64 = std::chrono::steady_clock::now();
-        Davidson<double> dv(c, nb, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
+        Davidson<double> dv(c, nbi, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
         dv.record_history(rec);
-        Q3B_CUDA(cudaMemcpyAsync(dv.V(), bands_dev, band_bytes, cudaMemcpyDeviceToDevice, c.stream));
+        Q3B_CUDA(cudaMemcpyAsync(dv.V(), mix, (size_t)npw * nbi * sizeof(double2), cudaMemcpyDeviceToDevice,
+                                 c.stream));
         const int sweeps = o.refine_sweeps > 0 ? o.refine_sweeps : std::max(1, o.max_iterations);
-        auto r = dv.solve(nb, eig32, o.tolerance, sweeps, occupied, bands_dev, true,
+        auto r = dv.solve(nbi, eig32, o.tolerance, sweeps, occupied, mix, true,
                           o.profile_stages ? s.stage_ms : nullptr);
-        std::copy(r.eig.begin(), r.eig.end(), eig_host);
+        Q3B_CUDA(cudaMemcpyAsync(bands_dev, mix, band_bytes, cudaMemcpyDeviceToDevice, c.stream));
+        std::copy(r.eig.begin(), r.eig.begin() + nb, eig_host);
         s.iterations = it32 + r.iterations;
         s.fp64_iterations = r.iterations;
         s.h_applications = h32 + dv.happly();
@@ -818,6 +853,7 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         s.max_residual_norm = r.resid;
         Q3B_CUDA(cudaStreamSynchronize(c.stream));
         s.fp64_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t64).count();
+        hist_width = nbi;
     } else {
         throw Status(Q3B_ERR_INVALID, "unknown precision");
     }
@@ -825,8 +861,11 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
     tc::check_error(c.stream);
     s.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (rec) {
-        const size_t rows = std::min(hist.size() / (size_t)nb, (size_t)o.history_rows);
-        std::copy(hist.begin(), hist.begin() + rows * nb, o.eigenvalue_history);
+        // rows of hist_width values (the mixed solve's buffer bands after the nb)
+        const size_t rows = std::min(hist.size() / (size_t)hist_width, (size_t)o.history_rows);
+        for (size_t i = 0; i < rows; ++i)
+            std::copy(hist.begin() + i * hist_width, hist.begin() + i * hist_width + nb,
+                      o.eigenvalue_history + i * nb);
     }
     if (stats) *stats = s;
 }

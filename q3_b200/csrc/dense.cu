@@ -927,6 +927,14 @@ size_t hegv_scratch_bytes(int n) {
            (size_t)n * sizeof(unsigned) + 64 * 1024;
 }
 
+bool order_supported(int n) {
+    if (n < 1) return false;
+    const int nsm = device_sms();
+    const int G = std::max(1, std::min(nsm, (n + 7) / 8));
+    const int cpb = (n + G - 1) / G;
+    return ((size_t)cpb * n + 3 * (size_t)n) * sizeof(double2) <= 200 * 1024;
+}
+
 int potrf(cudaStream_t st, int n, double2* A, int lda, Scratch& ws) {
     Chol c = chol_take(ws, n);
     return potrf_impl(st, n, A, lda, c);

@@ -127,6 +127,10 @@ int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, dou
          int nvec, Scratch& ws, const GemmWorkspace& gws, HegvGraphs* graphs = nullptr,
          double* w_host = nullptr);
 
+// Whether hegv/heev take a problem of order n on the current device (the
+// tridiagonalisation keeps its blocks' columns in shared memory).
+bool order_supported(int n);
+
 // Standard Hermitian eigenproblem of a full (both triangles) matrix A (n x n,
 // ld n; read only).  The lowest nvec eigenvalues ascending in w (all n when
 // nvec is 0), their eigenvectors in Z (ld n).

@@ -52,16 +52,22 @@ struct Job {
 // device bytes a solve of this size holds (vectors, subspace matrices and the
 // dense scratch, stick buffer, projectors, potential), with headroom
 size_t estimate_bytes(const Job& j) {
-    const size_t maxn = std::min<size_t>((size_t)std::max(2, j.opts.basis_expansion_factor) * j.nb, j.npw);
+    // the FP32 phase of a mixed solve holds a larger basis of 8-byte values, the
+    // FP64 solve (and the mixed refinement) a basis of 16-byte values: the larger
+    const bool mixed = j.opts.precision == Q3B_MIXED;
+    const size_t nbi = mixed ? (size_t)mixed_bands(j.nb, j.npw) : (size_t)j.nb;  // buffer bands of a mixed solve
+    const size_t maxn = std::min<size_t>((size_t)std::max(2, basis_factor(j.opts, j.nb, j.npw)) * nbi, j.npw);
+    const size_t maxn64 = std::min<size_t>((size_t)std::max(2, j.opts.basis_expansion_factor) * nbi, j.npw);
     const size_t N = (size_t)j.n1 * j.n2 * j.n3;
     size_t b = 0;
-    b += 3 * (size_t)j.npw * maxn * sizeof(double2);
+    b += 3 * (size_t)j.npw * std::max(maxn * (mixed ? sizeof(float2) : sizeof(double2)), maxn64 * sizeof(double2));
+    if (mixed) b += (size_t)j.npw * nbi * sizeof(double2);  // the bands between the two phases
     b += 10 * maxn * maxn * sizeof(double2) + dense::hegv_scratch_bytes((int)maxn) +
          dense::potrf_scratch_bytes((int)maxn);
     b += std::min<size_t>(48ull << 20, (size_t)j.nb * j.n3 * (size_t)j.n1 * j.n2 / 4 * sizeof(double2));
     // projectors: FP64, FP32 and the two packed tensor-core copies (16 B each)
     b += (size_t)j.npw * j.nproj * (sizeof(double2) + sizeof(float2) + 32);
-    b += N * (sizeof(double) + sizeof(float));
+    b += 2 * N * (sizeof(double) + sizeof(float));  // V/N in two layouts
     b += 2 * (size_t)j.nproj * j.nb * sizeof(double2) + (16ull << 20);
     return b + b / 5;
 }

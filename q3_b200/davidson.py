@@ -61,6 +61,10 @@ class PlanewaveDavidsonDiagonalizer:
         if refine_sweeps is not None:
             self.opts.refine_sweeps = int(refine_sweeps)
 
+    def set_mixed_expansion_factor(self, factor: int) -> None:
+        """Basis expansion factor of the mixed solve's FP32 phase (0: the library's choice)."""
+        self.opts.mixed_expansion_factor = int(factor)
+
     def set_occupied_bands(self, n: int) -> None:
         self.opts.occupied_bands = int(n)
 

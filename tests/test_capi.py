@@ -54,9 +54,9 @@ def test_davidson_default_opts_fill_every_field():
     o.tolerance, o.max_iterations, o.basis_expansion_factor = -1.0, -1, -1
     o.occupied_bands, o.precision, o.refine_sweeps = -1, -1, -1
     o.mixed_tolerance, o.profile_stages = -1.0, -1
-    o.eigenvalue_history, o.history_rows = 0x1234, 77
+    o.eigenvalue_history, o.history_rows, o.mixed_expansion_factor = 0x1234, 77, 9
     lib.q3b_davidson_default_opts(C.byref(o))
     assert o.tolerance == 1e-2 and o.max_iterations == 20 and o.basis_expansion_factor == 2
     assert o.occupied_bands == 0 and o.precision == _lib.FP64 and o.refine_sweeps == 0
     assert o.mixed_tolerance == 1e-6 and o.profile_stages == 0
-    assert not o.eigenvalue_history and o.history_rows == 0
+    assert not o.eigenvalue_history and o.history_rows == 0 and o.mixed_expansion_factor == 0

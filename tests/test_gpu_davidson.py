@@ -317,17 +317,19 @@ def test_davidson_eigenvalue_history(cuda_device, ctx_app, precision):
 
 
 def test_mixed_default_refinement_converges_slow_request(cuda_device, ctx_app):
-    """Request 18 of the serving stream (112 bands, npw 11,123, 60^3) needs 207 FP64 iterations;
-    its mixed solve needs over 100 refinement iterations.  With the default refinement budget (up
-    to max_iterations) it converges, within 1e-8 Ha of the FP64 solve."""
+    """Request 18 of the serving stream (112 bands, npw 11,123, 60^3) needs 207 FP64 iterations at
+    1e-9 Ry; at the reference's basis factor its mixed solve needed over 100 refinement
+    iterations.  With the default refinement budget (up to max_iterations) it converges, within
+    1e-8 Ha of an FP64 solve converged to 1e-11 Ry (two solves that each stop on a loose
+    eigenvalue-change test differ by both stopping errors)."""
     from q3_b200.davidson import PlanewaveDavidsonDiagonalizer
     sy = synthetic.serving_requests(19)[18]
     _prep(ctx_app, sy)
     res = {}
-    for prec in (FP64, MIXED):
+    for prec, tol in ((FP64, 1e-11), (MIXED, 1e-9)):
         d = PlanewaveDavidsonDiagonalizer(ctx_app, prec)
-        d.set_tolerance(1e-9)
-        d.set_maximum_iterations(300)
+        d.set_tolerance(tol)
+        d.set_maximum_iterations(400)
         res[prec] = d.solve(sy.psi0[0], sy.nbands)
     assert res[FP64].unconverged == 0
     assert res[MIXED].unconverged == 0
