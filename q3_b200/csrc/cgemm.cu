@@ -361,8 +361,12 @@ void zgemm_big_run(cudaStream_t st, dim3 grid, int M, int N, int K, double2 alph
                    const double2* B, long ldb, double2 beta, double2* C, long ldc, int kchunk, double2* part) {
     constexpr size_t smem = big::Shape<TM>::smem;
     static_assert(smem <= 227 * 1024, "zgemm_big stages exceed shared memory");
-    // the attribute is per function and device: set on every launch
-    Q3B_CUDA(cudaFuncSetAttribute(zgemm_big<CONJ_A, TM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // the attribute belongs to the function on one device
+    static PerDeviceOnce once;
+    once.run([] {
+        Q3B_CUDA(cudaFuncSetAttribute(zgemm_big<CONJ_A, TM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)big::Shape<TM>::smem));
+    });
     zgemm_big<CONJ_A, TM><<<grid, big::THREADS, smem, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kchunk,
                                                              part);
     Q3B_LAUNCH_CHECK();

@@ -444,22 +444,36 @@ template <typename R> class Davidson {
         const T* C = narrowed(basis, nb_, evec_, basis, evecR_);
         gemm(false, npw_, nb_, basis, one(), V_, npw_, C, basis, zero(), out, npw_);
         if (resid_max) {
-            std::vector<int> all(nb_);
-            std::iota(all.begin(), all.end(), 0);
-            upload_async(idx_, all.data(), nb_ * sizeof(int), st_);
-            pack_coefficients<R><<<grid_for((long)basis * nb_), 256, 0, st_>>>(basis, nb_, evec_, idx_, w_,
-                                                                               cpack_, cneg_, eps_);
-            Q3B_LAUNCH_CHECK();
-            gemm(false, npw_, nb_, basis, one(), SV_, npw_, cneg_, basis, zero(), tmp_, npw_);
-            gemm(false, npw_, nb_, basis, one(), HV_, npw_, cpack_, basis, one(), tmp_, npw_);
-            column_norms<R><<<nb_, 256, 0, st_>>>(npw_, tmp_, norms_, gamma_ ? 1 : 0);
-            Q3B_LAUNCH_CHECK();
-            double* h = static_cast<double*>(host_readback(nb_ * sizeof(double)));
-            Q3B_CUDA(cudaMemcpyAsync(h, norms_, nb_ * sizeof(double), cudaMemcpyDeviceToHost, st_));
-            Q3B_CUDA(cudaStreamSynchronize(st_));
-            *resid_max = *std::max_element(h, h + nb_);
+            const std::vector<double> r = residual_norms(basis);
+            *resid_max = *std::max_element(r.begin(), r.end());
         }
     }
+
+    // ||(HV) c_b - eps_b (SV) c_b|| of the current Ritz pairs, every band (on the host)
+    std::vector<double> residual_norms(int basis) {
+        std::vector<int> all(nb_);
+        std::iota(all.begin(), all.end(), 0);
+        upload_async(idx_, all.data(), nb_ * sizeof(int), st_);
+        pack_coefficients<R><<<grid_for((long)basis * nb_), 256, 0, st_>>>(basis, nb_, evec_, idx_, w_, cpack_,
+                                                                           cneg_, eps_);
+        Q3B_LAUNCH_CHECK();
+        gemm(false, npw_, nb_, basis, one(), SV_, npw_, cneg_, basis, zero(), tmp_, npw_);
+        gemm(false, npw_, nb_, basis, one(), HV_, npw_, cpack_, basis, one(), tmp_, npw_);
+        column_norms<R><<<nb_, 256, 0, st_>>>(npw_, tmp_, norms_, gamma_ ? 1 : 0);
+        Q3B_LAUNCH_CHECK();
+        double* h = static_cast<double*>(host_readback(nb_ * sizeof(double)));
+        Q3B_CUDA(cudaMemcpyAsync(h, norms_, nb_ * sizeof(double), cudaMemcpyDeviceToHost, st_));
+        Q3B_CUDA(cudaStreamSynchronize(st_));
+        return std::vector<double>(h, h + nb_);
+    }
+
+    // Residual gate of the mixed solve's refinement (0: off, the reference's test
+    // alone): when every band passes the eigenvalue-change test, the occupied bands
+    // whose squared residual norm exceeds the gate stay unconverged.  A band's
+    // eigenvalue error is at most about ||r||^2 / (its gap to the rest of the
+    // spectrum), while a slowly converging band can change by less than the
+    // tolerance per iteration and still be far from its limit.
+    void set_residual_gate(double g) { resid_gate_ = g; }
 
     // S|V> for columns [first, first+count): V + beta Q beta^H V (the
     // ultrasoft operator, overlap/pseudopotential/ultrasoft/init.hpp:189-345)
@@ -666,6 +680,12 @@ template <typename R> class Davidson {
             const bool stalled = stagnate && ((h >= 4 && history[h - 1] < kStallBelow &&
                                                history[h - 1] > 0.5 * history[h - 4]) ||
                                               since_low >= kFlatIterations);
+            if (unconv.empty() && !stalled && resid_gate_ > 0.0) {
+                const std::vector<double> r = residual_norms(basis);
+                for (int b = 0; b < occupied; ++b)
+                    if (r[b] * r[b] > resid_gate_) unconv.push_back(b);
+                res.unconverged = static_cast<int>(unconv.size());
+            }
             if (unconv.empty() || stalled) {                              // :649-668
                 res.stagnated = stalled && !unconv.empty();
                 extract(basis, out, want_resid ? &res.resid : nullptr);
@@ -749,6 +769,7 @@ template <typename R> class Davidson {
     std::vector<double> collapse_w_;
     std::vector<double> wread_;  // eigenvalues of the last subspace solve, on the host
     bool reuse_collapse_ = false;
+    double resid_gate_ = 0.0;
 };
 
 }  // namespace
@@ -807,12 +828,14 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         s.fp64_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     } else if (o.precision == Q3B_MIXED) {
         const int factor = basis_factor(o, nb, npw);
-        // Both phases solve for nbi = nb + a few buffer bands, held to the loose
-        // tolerance of empty bands; the lowest nb are returned.  Without them the
-        // block's top band, whose gap to the first band outside the block is small,
-        // converges so slowly in the refinement that its eigenvalue change can drop
-        // below the tolerance while it is still 1e-8 to 1e-7 Ry from its limit.
-        const int nbi = mixed_bands(nb, npw);
+        // With the larger basis, both phases solve for nbi = nb + a few buffer bands,
+        // held to the loose tolerance of empty bands; the lowest nb are returned.
+        // Without them the FP32 phase, which ends sooner with the larger basis, hands
+        // over a block whose top band (its gap to the first band outside the block
+        // is small) converges so slowly in the refinement that its eigenvalue change
+        // can drop below the tolerance while it is still 1e-8 to 1e-7 Ry from its
+        // limit.  At the reference's factor the solve is the plain two-phase one.
+        const int nbi = factor > o.basis_expansion_factor ? mixed_bands(nb, npw) : nb;
         c.ws_mixed.reserve(&c, (size_t)npw * nbi * sizeof(double2));
         double2* mix = c.ws_mixed.as<double2>();
         std::vector<double> stored_i(nbi, 0.0);
@@ -838,6 +861,8 @@ void davidson_solve(Context& c, double2* bands_dev, double* eig_host, int nb, co
         const auto t64 = std::chrono::steady_clock::now();
         Davidson<double> dv(c, nbi, o.basis_expansion_factor, c.ws_solver, c.ws_dense);
         dv.record_history(rec);
+        // a tenth of the tolerance: an eigenvalue within about tol / (10 gap) of its limit
+        dv.set_residual_gate(0.1 * o.tolerance);
         Q3B_CUDA(cudaMemcpyAsync(dv.V(), mix, (size_t)npw * nbi * sizeof(double2), cudaMemcpyDeviceToDevice,
                                  c.stream));
         const int sweeps = o.refine_sweeps > 0 ? o.refine_sweeps : std::max(1, o.max_iterations);

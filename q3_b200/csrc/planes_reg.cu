@@ -341,10 +341,14 @@ template <typename R, int N, int L> bool launch_one(const LocalPlan<R>& p, cplx_
         return false;
     const size_t smem = reg_plane_smem<R, N, L>(p);
     if (smem > 227 * 1024) return false;
-    // the attribute belongs to the function on the current device; setting it
-    // on every launch keeps it right on whichever device the context uses
-    Q3B_CUDA(cudaFuncSetAttribute(planes_reg<R, N, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(smem)));
+    // the attribute belongs to the function on one device: raised to the most
+    // any plane may ask for, once per device (contexts on other threads launch
+    // with other sizes at the same time, so it is never set to one launch's size)
+    static PerDeviceOnce once;
+    once.run([] {
+        Q3B_CUDA(cudaFuncSetAttribute(planes_reg<R, N, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      227 * 1024));
+    });
     planes_reg<R, N, L><<<dim3(p.n3, nb), reg_plane_threads<R, N, L>(), smem, st>>>(p, X, err);
     return true;
 }

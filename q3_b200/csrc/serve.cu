@@ -55,8 +55,10 @@ size_t estimate_bytes(const Job& j) {
     // the FP32 phase of a mixed solve holds a larger basis of 8-byte values, the
     // FP64 solve (and the mixed refinement) a basis of 16-byte values: the larger
     const bool mixed = j.opts.precision == Q3B_MIXED;
-    const size_t nbi = mixed ? (size_t)mixed_bands(j.nb, j.npw) : (size_t)j.nb;  // buffer bands of a mixed solve
-    const size_t maxn = std::min<size_t>((size_t)std::max(2, basis_factor(j.opts, j.nb, j.npw)) * nbi, j.npw);
+    const int factor = basis_factor(j.opts, j.nb, j.npw);
+    const size_t nbi = mixed && factor > j.opts.basis_expansion_factor ? (size_t)mixed_bands(j.nb, j.npw)
+                                                                       : (size_t)j.nb;  // buffer bands
+    const size_t maxn = std::min<size_t>((size_t)std::max(2, factor) * nbi, j.npw);
     const size_t maxn64 = std::min<size_t>((size_t)std::max(2, j.opts.basis_expansion_factor) * nbi, j.npw);
     const size_t N = (size_t)j.n1 * j.n2 * j.n3;
     size_t b = 0;

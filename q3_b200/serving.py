@@ -11,7 +11,7 @@ from __future__ import annotations
 import ctypes as C
 import dataclasses
 import time
-from typing import Dict, List, Optional, Sequence
+from typing import Dict, Iterable, List, Optional, Sequence
 
 import numpy as np
 
@@ -91,36 +91,20 @@ class BandSolveServer:
     def done(self, rid: int) -> bool:
         return self.lib.q3b_server_poll(self.h, rid) == 1
 
-    def wait(self, rid: int) -> Served:
+    def wait(self, rid: int, keep_bands: bool = True) -> Served:
+        """Block until request `rid` is done; its bands come back only with keep_bands."""
         npw, nb = self._shape.pop(rid)
-        bands = np.empty((npw, nb), dtype=np.complex128, order="F")
+        bands = np.empty((npw, nb), dtype=np.complex128, order="F") if keep_bands else None
         eig = np.empty(nb, dtype=np.float64)
         st = DavidsonStats()
         tm = RequestTimes()
-        self._check(self.lib.q3b_server_wait(self.h, rid, bands.ctypes.data, eig.ctypes.data,
-                                             C.byref(st), C.byref(tm)))
+        self._check(self.lib.q3b_server_wait(self.h, rid, bands.ctypes.data if keep_bands else None,
+                                             eig.ctypes.data, C.byref(st), C.byref(tm)))
         return Served(rid, eig, bands, st.iterations, st.fp64_iterations, st.unconverged,
                       tm.queue_ms, tm.solve_ms, tm.latency_ms, tm.estimated_bytes)
 
 
-def run_poisson_stream(server: BandSolveServer, systems: Sequence, rate_hz: float, seed: int = 1238,
-                       **solve_kw) -> Dict:
-    """Submit `systems` at seeded Poisson arrival times; collect every result.
-
-    Returns p50/p99 latency (ms), solves/s over the stream and the results."""
-    rng = np.random.default_rng(seed)
-    gaps = rng.exponential(1.0 / rate_hz, size=len(systems))
-    t0 = time.perf_counter()
-    ids: List[int] = []
-    next_t = 0.0
-    for sy, gap in zip(systems, gaps):
-        next_t += gap
-        delay = next_t - (time.perf_counter() - t0)
-        if delay > 0:
-            time.sleep(delay)
-        ids.append(server.submit(sy, **solve_kw))
-    results = [server.wait(i) for i in ids]
-    wall = time.perf_counter() - t0
+def _summary(results, wall: float) -> Dict:
     lat = np.array([r.latency_ms for r in results])
     return {
         "requests": len(results),
@@ -132,3 +116,66 @@ def run_poisson_stream(server: BandSolveServer, systems: Sequence, rate_hz: floa
         "unconverged_requests": int(sum(1 for r in results if r.unconverged)),
         "results": results,
     }
+
+
+def run_poisson_stream(server: BandSolveServer, systems: Iterable, rate_hz: float, seed: int = 1238,
+                       count: Optional[int] = None, keep_bands: bool = True, **solve_kw) -> Dict:
+    """Submit `systems` (a sequence, or an iterable of `count` systems built as they are
+    needed) at seeded Poisson arrival times; collect every result, finished ones as the
+    stream goes (without their bands unless keep_bands).
+
+    Returns p50/p99 latency (ms), solves/s over the stream and the results in order."""
+    n = len(systems) if count is None else int(count)
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate_hz, size=n)
+    t0 = time.perf_counter()
+    pending: List[int] = []
+    done: Dict[int, Served] = {}
+    order: List[int] = []
+    next_t = 0.0
+    for sy, gap in zip(systems, gaps):
+        next_t += gap
+        delay = next_t - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        rid = server.submit(sy, **solve_kw)
+        order.append(rid)
+        pending.append(rid)
+        still = []
+        for p in pending:
+            if server.done(p):
+                done[p] = server.wait(p, keep_bands)
+            else:
+                still.append(p)
+        pending = still
+    for p in pending:
+        done[p] = server.wait(p, keep_bands)
+    wall = time.perf_counter() - t0
+    return _summary([done[r] for r in order], wall)
+
+
+def run_closed_loop(server: BandSolveServer, systems: Iterable, window: int, keep_bands: bool = False,
+                    **solve_kw) -> Dict:
+    """Capacity: keep `window` requests in the server (queued or running), submitting the next
+    as one finishes, over all of `systems`; solves/s over the whole run."""
+    t0 = time.perf_counter()
+    inflight: List[int] = []
+    done: Dict[int, Served] = {}
+    order: List[int] = []
+    for sy in systems:
+        while len(inflight) >= window:
+            still = []
+            for p in inflight:
+                if server.done(p):
+                    done[p] = server.wait(p, keep_bands)
+                else:
+                    still.append(p)
+            inflight = still
+            if len(inflight) >= window:
+                time.sleep(0.0005)
+        rid = server.submit(sy, **solve_kw)
+        order.append(rid)
+        inflight.append(rid)
+    for p in inflight:
+        done[p] = server.wait(p, keep_bands)
+    return _summary([done[r] for r in order], time.perf_counter() - t0)

@@ -366,15 +366,34 @@ def request_cell(rng: np.random.Generator) -> Tuple[Cell, int]:
     return cell, 4 * n
 
 
-def serving_requests(count: int, seed: int = 1238) -> List[System]:
-    """The request stream of the serving configuration (cells only; arrivals apart)."""
+@dataclasses.dataclass
+class RequestSpec:
+    """What one serving request is built from (its cell, band count and seed)."""
+    name: str
+    cell: Cell
+    nbands: int
+    seed: int
+
+
+def serving_request_specs(count: int, seed: int = 1238) -> List[RequestSpec]:
+    """The cells of the serving stream's first `count` requests, drawn in order from one
+    seeded stream (cheap: the inputs themselves are built by build_request)."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
         cell, nb = request_cell(rng)
-        out.append(build_system(f"request{i}", cell, np.zeros((1, 3)), nb,
-                                int(rng.integers(0, 2 ** 31))))
+        out.append(RequestSpec(f"request{i}", cell, nb, int(rng.integers(0, 2 ** 31))))
     return out
+
+
+def build_request(spec: RequestSpec) -> System:
+    """The inputs of one serving request (Gamma point)."""
+    return build_system(spec.name, spec.cell, np.zeros((1, 3)), spec.nbands, spec.seed)
+
+
+def serving_requests(count: int, seed: int = 1238) -> List[System]:
+    """The request stream of the serving configuration (cells only; arrivals apart)."""
+    return [build_request(s) for s in serving_request_specs(count, seed)]
 
 
 @dataclasses.dataclass
