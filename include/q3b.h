@@ -73,6 +73,17 @@ size_t q3b_device_bytes(const q3b_context* ctx);
  * The 1/N scaling of the reference's cached potential is applied inside. */
 int q3b_set_potential(q3b_context* ctx, const double* v_r_host, int n1, int n2, int n3);
 
+/* update_potential when the density grid is larger than the wavefunction grid
+ * (serial.hpp:64-78 -> compute_smooth_grid_potential_from_dense and
+ * inverse_fft_smooth_potential, planewave_potential_utils.hpp:33-135): V(r) on
+ * the density grid d1 x d2 x d3 (flat (i1*d2+i2)*d3+i3, Ry) is restricted to the
+ * wavefunction grid n1 x n2 x n3 by G-space truncation (forward transform, the
+ * coefficients of Miller indices -n/2 < m <= n/2 per axis, inverse transform,
+ * real part) on the device, then taken as q3b_set_potential takes it.  Each
+ * n_i must be at most d_i; equal grids are the identity. */
+int q3b_set_potential_dense(q3b_context* ctx, const double* v_dense_host, int d1, int d2, int d3, int n1,
+                            int n2, int n3);
+
 /* invalidate_smooth_potential_cache (init.hpp:90) / is_smooth_potential_cache_valid (:96) */
 int q3b_invalidate_potential(q3b_context* ctx);
 int q3b_potential_valid(const q3b_context* ctx);

@@ -26,6 +26,28 @@ def _workers(threads: Optional[int]) -> int:
     return max(1, int(threads))
 
 
+def restrict_potential(v_dense: np.ndarray, dense_grid, smooth_grid) -> np.ndarray:
+    """V(r) on the wavefunction grid from V(r) on the larger density grid by G-space truncation
+    (compute_smooth_grid_potential_from_dense, planewave_potential_utils.hpp:33-104, and
+    inverse_fft_smooth_potential, :110-135): forward transform on the density grid divided by
+    its point count, the coefficients of every wrapped wavefunction-grid index w taken at Miller
+    index m = w (w <= n/2) or w - n (so +n/2 is the Nyquist representative), an unnormalised
+    inverse transform on the wavefunction grid, the real part.  Flat (i1*N2 + i2)*N3 + i3 in and
+    out."""
+    d = tuple(int(x) for x in dense_grid)
+    n = tuple(int(x) for x in smooth_grid)
+    if d == n:
+        return np.asarray(v_dense, dtype=np.float64).copy()          # serial.hpp:857-859
+    vg = np.fft.fftn(np.asarray(v_dense, dtype=np.float64).reshape(d)) / float(np.prod(d))
+    idx = []
+    for ni, di in zip(n, d):
+        w = np.arange(ni)
+        m = np.where(w <= ni // 2, w, w - ni)
+        idx.append(np.mod(m, di))
+    vs = vg[np.ix_(*idx)]
+    return np.ascontiguousarray((np.fft.ifftn(vs) * float(np.prod(n))).real.reshape(-1))
+
+
 def scaled_potential(v_r: np.ndarray) -> np.ndarray:
     """serial.hpp:64-78: the cached potential is V(r) / N."""
     return np.asarray(v_r, dtype=np.float64) * (1.0 / v_r.size)

@@ -108,14 +108,18 @@ template <typename T> std::vector<T> read_array(const std::string& path, std::si
 
 // --------------------------------------------------------- forced FFT grids
 
+// The wavefunction grid n1 x n2 x n3 and the density grid d1 x d2 x d3 (the same
+// unless the case names a larger one: update_potential then restricts V(r) from
+// the density grid to the wavefunction grid, serial.hpp:64-78, 853-870).
 class ForcedGridFactory : public FFTGridFactory {
   public:
-    ForcedGridFactory(int n1, int n2, int n3) : n1_(n1), n2_(n2), n3_(n3) {}
+    ForcedGridFactory(int n1, int n2, int n3, int d1, int d2, int d3)
+        : n1_(n1), n2_(n2), n3_(n3), d1_(d1), d2_(d2), d3_(d3) {}
     std::unique_ptr<FFTGrid> create_fft_grid() const override {
         return std::make_unique<Forced>(n1_, n2_, n3_);
     }
     std::unique_ptr<FFTGrid> create_density_fft_grid() const override {
-        return std::make_unique<Forced>(n1_, n2_, n3_);
+        return std::make_unique<Forced>(d1_, d2_, d3_);
     }
 
   private:
@@ -128,7 +132,7 @@ class ForcedGridFactory : public FFTGridFactory {
       private:
         int n1_, n2_, n3_;
     };
-    int n1_, n2_, n3_;
+    int n1_, n2_, n3_, d1_, d2_, d3_;
 };
 
 // ------------------------------------------------------- synthetic species
@@ -203,7 +207,10 @@ int main(int argc, char** argv) {
         const std::string out = argv[2];
         const int n1 = c.integer("grid", 0), n2 = c.integer("grid", 1), n3 = c.integer("grid", 2);
         const double alat = c.num("alat");
-        ForcedGridFactory grids(n1, n2, n3);
+        const bool dense = c.has("density_grid");
+        const int d1 = dense ? c.integer("density_grid", 0) : n1, d2 = dense ? c.integer("density_grid", 1) : n2,
+                  d3 = dense ? c.integer("density_grid", 2) : n3;
+        ForcedGridFactory grids(n1, n2, n3, d1, d2, d3);
 
         // --- crystal: lattice rows in bohr, atoms fractional, one species
         Crystal crystal;
@@ -246,7 +253,8 @@ int main(int argc, char** argv) {
 
         // --- potential V(r), flat (i1*N2 + i2)*N3 + i3, Ry
         const std::size_t N = static_cast<std::size_t>(n1) * n2 * n3;
-        std::vector<Real> v_r = read_array<double>(c.str("potential"), N);
+        // V(r) on the density grid, flat (i1*D2 + i2)*D3 + i3
+        std::vector<Real> v_r = read_array<double>(c.str("potential"), static_cast<std::size_t>(d1) * d2 * d3);
 
         // --- beta(q) tables exactly as the reference tabulates them
         {

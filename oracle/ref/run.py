@@ -45,20 +45,25 @@ def d_channels_of(system) -> np.ndarray:
 def write_case(system, workdir: Path, mode: str = "setup", *, hpsi_vectors: int = 0,
                hpsi_repeats: int = 1, tolerance: float = 1e-10, max_iterations: int = 200,
                davidson_kpoints: Sequence[int] = (0,), dump_projectors: bool = False,
-               nbands: Optional[int] = None) -> Path:
+               nbands: Optional[int] = None, dense_potential: Optional[np.ndarray] = None,
+               density_grid: Optional[Sequence[int]] = None) -> Path:
     from q3_b200 import synthetic
     workdir.mkdir(parents=True, exist_ok=True)
     cell = system.cell
     lat = np.asarray(cell.lattice, dtype=np.float64)
     alat = float(np.linalg.norm(lat[0])) if np.allclose(lat, np.diag(np.diag(lat))) else float(
         2.0 * abs(lat[0, 1]))
-    system.v_r.astype(np.float64).tofile(workdir / "v_r.f64")
+    # V(r) on the density grid when one is given (the reference restricts it), else on
+    # the wavefunction grid
+    v = system.v_r if dense_potential is None else dense_potential
+    np.asarray(v, dtype=np.float64).tofile(workdir / "v_r.f64")
     d = d_channels_of(system)
     lines = [
         "# written by oracle/ref/run.py",
         f"alat {alat!r}",
         "lattice " + " ".join(repr(float(x)) for x in lat.reshape(-1)),
         "grid {} {} {}".format(*cell.grid),
+        *(["density_grid {} {} {}".format(*density_grid)] if density_grid is not None else []),
         f"ecutwfc {float(cell.ecut_ry)!r}",
         f"valence {VALENCE!r}",
         f"mesh {MESH_XMIN!r} {MESH_DX!r} {MESH_POINTS}",

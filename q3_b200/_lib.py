@@ -91,6 +91,7 @@ SIGNATURES = {
     "q3b_synchronize": (_i, [_vp]),
     "q3b_device_bytes": (_sz, [_vp]),
     "q3b_set_potential": (_i, [_vp, _vp, _i, _i, _i]),
+    "q3b_set_potential_dense": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i]),
     "q3b_invalidate_potential": (_i, [_vp]),
     "q3b_potential_valid": (_i, [_vp]),
     "q3b_prepare_kpoint": (_i, [_vp, _i, _vp, _vp, _vp, _i, _i, _vp, _vp]),

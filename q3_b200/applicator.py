@@ -87,12 +87,20 @@ class PlanewaveHamiltonianApplicator:
         self._keep = []
 
     # init.hpp:40
-    def update_potential(self, real_space_potential: np.ndarray, grid) -> None:
+    def update_potential(self, real_space_potential: np.ndarray, grid, density_grid=None) -> None:
+        """V(r) (Ry) on the wavefunction grid `grid`, or on a larger `density_grid`, from
+        which it is restricted to `grid` (the reference's dense-to-smooth step)."""
         v = np.ascontiguousarray(real_space_potential, dtype=np.float64)
         n1, n2, n3 = (int(x) for x in grid)
-        if v.size != n1 * n2 * n3:
-            raise ValueError("potential size does not match the grid")
-        check(self.h, self.lib.q3b_set_potential(self.h, _ptr(v), n1, n2, n3))
+        if density_grid is None:
+            if v.size != n1 * n2 * n3:
+                raise ValueError("potential size does not match the grid")
+            check(self.h, self.lib.q3b_set_potential(self.h, _ptr(v), n1, n2, n3))
+        else:
+            d1, d2, d3 = (int(x) for x in density_grid)
+            if v.size != d1 * d2 * d3:
+                raise ValueError("potential size does not match the density grid")
+            check(self.h, self.lib.q3b_set_potential_dense(self.h, _ptr(v), d1, d2, d3, n1, n2, n3))
         self.grid = (n1, n2, n3)
 
     # init.hpp:90, :96

@@ -101,6 +101,10 @@ int q3b_set_potential(q3b_context* ctx, const double* v, int n1, int n2, int n3)
     return guarded(ctx, [&](Context& c) { c.set_potential(v, n1, n2, n3); });
 }
 
+int q3b_set_potential_dense(q3b_context* ctx, const double* v, int d1, int d2, int d3, int n1, int n2, int n3) {
+    return guarded(ctx, [&](Context& c) { c.set_potential_dense(v, d1, d2, d3, n1, n2, n3); });
+}
+
 int q3b_invalidate_potential(q3b_context* ctx) {
     return guarded(ctx, [&](Context& c) { c.pot_valid = false; });
 }

@@ -238,6 +238,91 @@ void Context::set_potential(const double* v, int a, int b, int c) {
     kp.lp32.vnat = v32nat.as<float>();
 }
 
+// ---------------------------------------------------- dense -> smooth potential
+// in[a][b][c] (c fastest) -> out[c][a][b], complex in; real part out when re_out
+__global__ void rotate_axes(int A, int B, int Cn, const double2* __restrict__ in, double2* out, double* re_out) {
+    const long n = (long)A * B * Cn;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int c = static_cast<int>(i % Cn);
+        const long ab = i / Cn;
+        const double2 v = in[i];
+        const long o = (long)c * A * B + ab;  // ab = a*B + b
+        if (re_out) re_out[o] = v.x;
+        else out[o] = v;
+    }
+}
+
+// R (n x d, column-major): the restriction of one axis, x -> F_n^-1 P F_d x / d with
+// P keeping Miller indices m = w (w <= n/2) or w - n of the n wrapped indices w (the
+// +n/2 Nyquist representative, planewave_potential_utils.hpp:69-99):
+//   R[w, j] = (1/d) sum_m exp(2 pi i m (w/n - j/d)), in long double
+static std::vector<double2> restriction_matrix(int n, int d) {
+    std::vector<double2> R((size_t)n * d);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int w = 0; w < n; ++w)
+        for (int j = 0; j < d; ++j) {
+            long double re = 0.0L, im = 0.0L;
+            for (int wp = 0; wp < n; ++wp) {
+                const int m = wp <= n / 2 ? wp : wp - n;
+                const long double ang = two_pi * m * ((long double)w / n - (long double)j / d);
+                re += cosl(ang);
+                im += sinl(ang);
+            }
+            R[(size_t)j * n + w] = make_double2(static_cast<double>(re / d), static_cast<double>(im / d));
+        }
+    return R;
+}
+
+// update_potential with V(r) on a density grid larger than the wavefunction grid
+// (serial.hpp:64-78 with compute_smooth_grid_potential_from_dense and
+// inverse_fft_smooth_potential, planewave_potential_utils.hpp:33-135).  The 3D
+// truncation is the product of one restriction per axis, applied as three FP64
+// complex GEMMs with an axis rotation after each; the real part is V on the
+// wavefunction grid, which then goes through set_potential.
+void Context::set_potential_dense(const double* v, int d1, int d2, int d3, int a, int b, int c) {
+    if (!v || d1 <= 0 || d2 <= 0 || d3 <= 0 || a <= 0 || b <= 0 || c <= 0 || a > d1 || b > d2 || c > d3)
+        throw Status(Q3B_ERR_INVALID, "bad density / wavefunction grids (each wavefunction dimension must be "
+                                      "positive and at most the density grid's)");
+    if (a == d1 && b == d2 && c == d3) {  // the same grid: the restriction is the identity
+        set_potential(v, a, b, c);
+        return;
+    }
+    const size_t Nd = (size_t)d1 * d2 * d3;
+    std::vector<double2> vd(Nd);
+    for (size_t i = 0; i < Nd; ++i) vd[i] = make_double2(v[i], 0.0);
+    const auto R1 = restriction_matrix(a, d1), R2 = restriction_matrix(b, d2), R3 = restriction_matrix(c, d3);
+    DevBuf x, y, r1, r2, r3, vs;
+    // every stage holds at most Nd points (c*d1*d2, b*c*d1, a*b*c <= d1*d2*d3)
+    upload(this, x, vd.data(), Nd);
+    y.reserve(this, Nd * sizeof(double2));
+    upload(this, r1, R1.data(), R1.size());
+    upload(this, r2, R2.data(), R2.size());
+    upload(this, r3, R3.data(), R3.size());
+    vs.reserve(this, (size_t)a * b * c * sizeof(double));
+    const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
+    const GemmWorkspace none{};
+    auto blocks = [](long n) { return stride_grid(n, 8); };
+    // axis 3: [i1][i2][i3] -> [i1][i2][w3], then [w3][i1][i2]
+    cgemm<double>(stream, false, c, d1 * d2, d3, one, r3.as<double2>(), c, x.as<double2>(), d3, zero,
+                  y.as<double2>(), c, none);
+    rotate_axes<<<blocks((long)d1 * d2 * c), 256, 0, stream>>>(d1, d2, c, y.as<double2>(), x.as<double2>(), nullptr);
+    Q3B_LAUNCH_CHECK();
+    // axis 2: -> [w3][i1][w2], then [w2][w3][i1]
+    cgemm<double>(stream, false, b, c * d1, d2, one, r2.as<double2>(), b, x.as<double2>(), d2, zero,
+                  y.as<double2>(), b, none);
+    rotate_axes<<<blocks((long)c * d1 * b), 256, 0, stream>>>(c, d1, b, y.as<double2>(), x.as<double2>(), nullptr);
+    Q3B_LAUNCH_CHECK();
+    // axis 1: -> [w2][w3][w1], then [w1][w2][w3], real part
+    cgemm<double>(stream, false, a, b * c, d1, one, r1.as<double2>(), a, x.as<double2>(), d1, zero,
+                  y.as<double2>(), a, none);
+    rotate_axes<<<blocks((long)b * c * a), 256, 0, stream>>>(b, c, a, y.as<double2>(), nullptr, vs.as<double>());
+    Q3B_LAUNCH_CHECK();
+    std::vector<double> host((size_t)a * b * c);
+    Q3B_CUDA(cudaMemcpyAsync(host.data(), vs.ptr, host.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    Q3B_CUDA(cudaStreamSynchronize(stream));
+    set_potential(host.data(), a, b, c);
+}
+
 template <typename T, typename R> static std::vector<T> twiddles(int n) {
     std::vector<T> t(n);
     for (int m = 0; m < n; ++m) {

@@ -108,6 +108,8 @@ class Context {
     ~Context();
 
     void set_potential(const double* v, int a, int b, int c);
+    // V(r) on a density grid d1 x d2 x d3 restricted to the wavefunction grid a x b x c
+    void set_potential_dense(const double* v, int d1, int d2, int d3, int a, int b, int c);
     void prepare_kpoint(int npw, const int32_t* g2g, const double* ke, const double2* beta, int nproj,
                         int natoms, const int32_t* offs, const double* dblk, bool beta_on_device = false);
     void require_ready() const;

@@ -17,11 +17,12 @@ SKETCH_SEED = 20240601
 SKETCH_COLUMNS = 8
 
 
-def path(cid: int) -> Path:
+def path(cid) -> Path:
+    """cid: a configuration number, or a string such as "0_dense" for a variant fixture."""
     return HERE / f"ref_config{cid}.npz"
 
 
-def load(cid: int):
+def load(cid):
     return np.load(path(cid))
 
 
@@ -33,6 +34,24 @@ def system(cid: int):
 def sketch_columns(npw: int) -> np.ndarray:
     rng = np.random.default_rng(SKETCH_SEED)
     return rng.choice([-1.0, 1.0], size=(npw, SKETCH_COLUMNS)).astype(np.complex128)
+
+
+DENSE_GRID = (48, 36, 40)
+DENSE_SEED = 20240602
+
+
+def dense_potential(sy, dense_grid=DENSE_GRID) -> np.ndarray:
+    """A seeded V(r) (Ry) on a density grid larger than the wavefunction grid: the smooth
+    synthetic potential's Fourier content plus components that only the density grid holds,
+    flat (i1*D2 + i2)*D3 + i3."""
+    d = tuple(int(x) for x in dense_grid)
+    rng = np.random.default_rng(DENSE_SEED)
+    v = 0.25 * rng.standard_normal(d)
+    x = [np.arange(di) / di for di in d]
+    r = np.meshgrid(*x, indexing="ij")
+    v += -1.5 * np.exp(-((np.sin(np.pi * r[0]) ** 2 + np.sin(np.pi * r[1]) ** 2
+                          + np.sin(np.pi * r[2]) ** 2) / 0.15))
+    return np.ascontiguousarray(v.reshape(-1))
 
 
 def v_checksum(v_r: np.ndarray) -> np.ndarray:

@@ -103,6 +103,46 @@ def test_config0_davidson(cuda_device):
     assert np.max(np.abs(mixed.eigenvalues - g["eig_tol12"])) < MIXED_EIG_TOL_RY
 
 
+def test_config0_dense_potential(cuda_device):
+    # V(r) on a 48x36x40 density grid, restricted on the device (q3b_set_potential_dense)
+    if not RF.path("0_dense").exists():
+        pytest.skip("ref_config0_dense.npz not generated")
+    gd = RF.load("0_dense")
+    g = _need(0)
+    sy = RF.system(0)
+    rk = RF.kpoint(sy, g)
+    ap = _applicator()
+    ap.update_potential(RF.dense_potential(sy, tuple(gd["density_grid"])), sy.cell.grid,
+                        density_grid=tuple(gd["density_grid"]))
+    ap.prepare_kpoint(0, rk.npw, rk.g_to_grid, rk.ke, np.asfortranarray(g["beta"]),
+                      rk.atom_proj_offsets, rk.d_blocks)
+    assert _rel(_apply(ap, rk.psi0), gd["hpsi"]) < FP64_TOL
+    assert _rel(_apply(ap, rk.psi0, MIXED), gd["hpsi"]) < FP32_TOL
+
+
+@pytest.mark.parametrize("dense", [(25, 31, 50), (24, 30, 27), (64, 64, 64), (24, 24, 24)])
+def test_dense_potential_matches_oracle(cuda_device, dense):
+    from oracle import hpsi as ohpsi
+    from q3_b200 import synthetic
+    sy = synthetic.small_system(nbands=4, seed=3, grid=(24, 24, 24), a=10.26, ecut=30.0, natoms=2)
+    vd = RF.dense_potential(sy, dense)
+    ap = _applicator()
+    ap.update_potential(vd, sy.cell.grid, density_grid=dense)
+    ap.prepare_system_kpoint(sy)
+    vs = ohpsi.restrict_potential(vd, dense, sy.cell.grid)
+    want = ohpsi.apply_h(sy.psi0[0], sy.kpoints[0], vs, sy.cell.grid)
+    assert _rel(_apply(ap, sy.psi0[0]), want) < FP64_TOL
+
+
+def test_dense_potential_rejects_a_smaller_density_grid(cuda_device):
+    from q3_b200._lib import Q3BError
+    ap = _applicator()
+    with pytest.raises(Q3BError):
+        ap.update_potential(np.zeros(20 * 24 * 24), (24, 24, 24), density_grid=(20, 24, 24))
+    with pytest.raises(ValueError):
+        ap.update_potential(np.zeros(10), (24, 24, 24), density_grid=(32, 32, 32))
+
+
 # ------------------------------------------------------- configs 1 and 3: H|psi>
 
 @pytest.mark.parametrize("cid", [1, 3])

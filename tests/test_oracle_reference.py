@@ -105,3 +105,44 @@ def test_config2_kpoint_davidson_matches_reference():
                      sy.nbands, 1e-10, max_iterations=300)
     assert res.iterations == int(g["iterations_tol10"][k])
     assert np.max(np.abs(res.eigenvalues - g["eig_tol10"][k])) < 1e-11
+
+
+def test_config0_dense_potential_matches_reference():
+    # V(r) given on a 48x36x40 density grid: the reference restricts it to the 24^3
+    # wavefunction grid by G-space truncation before it applies H
+    if not RF.path("0_dense").exists():
+        pytest.skip("ref_config0_dense.npz not generated")
+    g = RF.load("0_dense")
+    sy = RF.system(0)
+    vd = RF.dense_potential(sy, tuple(g["density_grid"]))
+    assert np.allclose(RF.v_checksum(vd), g["v_dense_checksum"], rtol=1e-13, atol=0)
+    vs = ohpsi.restrict_potential(vd, tuple(g["density_grid"]), sy.cell.grid)
+    assert np.max(np.abs(ohpsi.scaled_potential(vs) - g["v_scaled"])) / np.max(np.abs(g["v_scaled"])) < 1e-13
+    g0 = _need(0)
+    rk = _kp_with_beta(RF.kpoint(sy, g0), np.asfortranarray(g0["beta"]))
+    assert np.array_equal(RF.perm_of(g), RF.perm_of(g0))
+    got = ohpsi.apply_h(rk.psi0, rk, vs, sy.cell.grid)
+    assert np.max(np.abs(got - g["hpsi"])) / np.max(np.abs(g["hpsi"])) < 1e-13
+
+
+@pytest.mark.parametrize("dense,smooth", [((48, 36, 40), (24, 24, 24)), ((25, 31, 50), (20, 24, 27)),
+                                          ((16, 16, 16), (16, 16, 16))])
+def test_restriction_keeps_band_limited_potentials(dense, smooth):
+    # a V(r) whose Fourier components all lie strictly inside the wavefunction grid's
+    # Miller range is sampled, not changed, by the restriction
+    rng = np.random.default_rng(7)
+    r = np.meshgrid(*[np.arange(d) / d for d in dense], indexing="ij")
+    v = np.full(dense, 0.3)
+    for _ in range(6):
+        m = [int(rng.integers(-((n - 1) // 2), (n - 1) // 2 + 1)) for n in smooth]
+        ph = 2 * np.pi * sum(mi * ri for mi, ri in zip(m, r))
+        v += rng.normal() * np.cos(ph + rng.uniform(0, 2 * np.pi))
+    got = ohpsi.restrict_potential(v.reshape(-1), dense, smooth)
+    rs = np.meshgrid(*[np.arange(n) / n for n in smooth], indexing="ij")
+    rng = np.random.default_rng(7)
+    want = np.full(smooth, 0.3)
+    for _ in range(6):
+        m = [int(rng.integers(-((n - 1) // 2), (n - 1) // 2 + 1)) for n in smooth]
+        ph = 2 * np.pi * sum(mi * ri for mi, ri in zip(m, rs))
+        want += rng.normal() * np.cos(ph + rng.uniform(0, 2 * np.pi))
+    assert np.max(np.abs(got - want.reshape(-1))) < 1e-12
