@@ -57,12 +57,14 @@ def parse():
                     help="Poisson streams per precision (medians reported)")
     ap.add_argument("--serving-rate", type=float, default=0.0,
                     help="arrivals per second (default: 80%% of the measured FP64 capacity)")
-    ap.add_argument("--probe", choices=["mixed", "fp64", "hegv", "density", "precision"], default=None,
+    ap.add_argument("--probe", choices=["mixed", "fp64", "hegv", "density", "precision", "serving"],
+                    default=None,
                     help="profiling aid: apply H to the bench block three times in one precision "
                          "(after the plane-kernel tuning), run the subspace eigensolver on "
                          "random problems of the --hegv-orders (hegv), or accumulate the charge "
-                         "density of --density-bands bands of the bench cell (density), and exit; "
-                         "prints no bench line")
+                         "density of --density-bands bands of the bench cell (density), run the "
+                         "converged precision study (precision) or the config-4 request stream "
+                         "alone (serving), and exit; prints no bench line")
     ap.add_argument("--density-bands", type=int, default=39,
                     help="bands for --probe density (39: one stick chunk of the 80^3 cell in FP64)")
     ap.add_argument("--hegv-orders", default="16,32,64,96,128,192,256,384,512",
@@ -1033,6 +1035,9 @@ def run_probe(args):
         return
     if args.probe == "precision":
         print(json.dumps({"probe": "precision", "study": precision_study_section(0)}), flush=True)
+        return
+    if args.probe == "serving":
+        print(json.dumps({"probe": "serving", "config4_serving": config4_section(args)}), flush=True)
         return
     import torch
     from q3_b200 import synthetic

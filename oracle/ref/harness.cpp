@@ -17,14 +17,15 @@
 //   * PlanewaveDavidsonDiagonalizer::solve (diagonalizer/planewave/davidson.hpp:324-841).
 //
 // The FFT grids are forced to the case's N1 x N2 x N3 (a grid factory whose grids ignore the
-// sizer), both the wavefunction and the density grid, so the dense-to-smooth restriction is
-// the identity (serial.hpp:64-78 with planewave_potential_utils.hpp's equal-grid case).
+// sizer).  The density grid is the same grid unless the case names a larger one
+// ("density_grid D1 D2 D3"); V(r) is then given on that grid and update_potential restricts
+// it to the wavefunction grid (serial.hpp:64-78, planewave_potential_utils.hpp:33-135).
 //
 // The species: beta_l(r) = r^l exp(-r^2/w^2) given as r*beta on a logarithmic radial mesh,
 // D diagonal (Ry); the reference tabulates beta(q) by its own spherical Bessel transform.
 //
 // Usage: harness CASE_FILE OUT_DIR
-// The case file is "key value..." lines (see tests/golden/ref_cases.py, which writes them).
+// The case file is "key value..." lines (oracle/ref/run.py, write_case, writes them).
 #include <algorithm>
 #include <chrono>
 #include <cmath>

@@ -28,6 +28,8 @@
 namespace q3b {
 namespace {
 
+template <typename V> void release(V& v) { V().swap(v); }
+
 double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -178,6 +180,14 @@ class Server {
             c.set_potential(j.v.data(), j.n1, j.n2, j.n3);
             c.prepare_kpoint(j.npw, j.g2g.data(), j.ke.data(), j.nproj ? j.beta.data() : nullptr, j.nproj,
                              j.natoms, j.nproj ? j.offs.data() : nullptr, j.nproj ? j.dblk.data() : nullptr);
+            // the inputs now live on the device: release their host copies, so that a
+            // long stream holds host memory only for queued requests and results
+            release(j.v);
+            release(j.g2g);
+            release(j.ke);
+            release(j.beta);
+            release(j.offs);
+            release(j.dblk);
             const size_t bytes = (size_t)j.npw * j.nb * sizeof(double2);
             c.ws_bands.reserve(&c, bytes);
             Q3B_CUDA(cudaMemcpyAsync(c.ws_bands.ptr, j.bands.data(), bytes, cudaMemcpyHostToDevice, c.stream));
