@@ -102,6 +102,14 @@ int q3b_prepare_kpoint(q3b_context* ctx, int npw, const int32_t* g_to_grid_host,
                        int natoms, const int32_t* atom_proj_offsets_host,
                        const double* d_blocks_host);
 
+/* set_spin_channel (init.hpp:75-80): the D blocks of the prepared k-point for
+ * another spin channel, packed as d_blocks_host of q3b_prepare_kpoint (the
+ * same atoms and projector offsets; entries |D| <= 1e-15 dropped).  The
+ * reference reads D_ij(spin) when it rebuilds its block D after a channel
+ * change (serial.hpp:602-647); the channel's V(r) comes through
+ * q3b_set_potential as in the reference.  The projectors stay on the device. */
+int q3b_set_d_blocks(q3b_context* ctx, const double* d_blocks_host);
+
 /* apply_batch (init.hpp:59-61; serial.hpp:110-155): hpsi = H psi for nvec
  * vectors, device pointers, FP64 in and out.  precision Q3B_MIXED runs the
  * transforms and projector products in FP32 (inputs rounded, outputs widened).

@@ -211,6 +211,12 @@ class PlanewaveHamiltonianApplicator:
                                             int(precision))
         check(self.h, rc)
 
+    def set_d_blocks(self, d_blocks: np.ndarray) -> None:
+        """The D blocks of another spin channel (set_spin_channel, init.hpp:75-80), packed like
+        those given to prepare_kpoint; the projectors stay on the device."""
+        d = np.ascontiguousarray(d_blocks, dtype=np.float64)
+        check(self.h, self.lib.q3b_set_d_blocks(self.h, _ptr(d)))
+
     # UltrasoftPseudopotentialOverlapOperator (overlap/pseudopotential/ultrasoft/init.hpp)
     def set_overlap_blocks(self, q_blocks: np.ndarray) -> None:
         """Per-atom q_ij blocks, packed like the D blocks of the prepared k-point."""

@@ -105,6 +105,10 @@ int q3b_set_potential_dense(q3b_context* ctx, const double* v, int d1, int d2, i
     return guarded(ctx, [&](Context& c) { c.set_potential_dense(v, d1, d2, d3, n1, n2, n3); });
 }
 
+int q3b_set_d_blocks(q3b_context* ctx, const double* d_blocks_host) {
+    return guarded(ctx, [&](Context& c) { c.set_d_blocks(d_blocks_host); });
+}
+
 int q3b_invalidate_potential(q3b_context* ctx) {
     return guarded(ctx, [&](Context& c) { c.pot_valid = false; });
 }

@@ -613,6 +613,18 @@ void Context::set_overlap_blocks(const double* qblk) {
     kp.has_q = true;
 }
 
+// D blocks packed as at prepare_kpoint, for the same atoms and offsets
+void Context::set_d_blocks(const double* dblk) {
+    require_ready();
+    if (kp.nproj <= 0) throw Status(Q3B_ERR_STATE, "the k-point has no projectors");
+    if (!dblk) throw Status(Q3B_ERR_INVALID, "null D blocks");
+    std::vector<double> d64(kp.dpk_len);
+    for (size_t i = 0; i < kp.dpk_len; ++i) d64[i] = std::fabs(dblk[i]) > 1e-15 ? dblk[i] : 0.0;
+    std::vector<float> d32(d64.begin(), d64.end());
+    upload(this, kp.dpk64, d64.data(), d64.size());
+    upload(this, kp.dpk32, d32.data(), d32.size());
+}
+
 template <typename R> int Context::sticks_chunk(int nvec) const {
     const size_t per = sticks_bytes_per_band(local_plan<R>());
     const size_t target = 48ull << 20;  // keep a chunk's sticks resident in L2

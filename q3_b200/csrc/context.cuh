@@ -119,6 +119,8 @@ class Context {
     // the same projectors with the ultrasoft overlap blocks Q in place of D
     template <typename R> NonlocalData<R> overlap() const;
     void set_overlap_blocks(const double* qblk);
+    // the D blocks of the prepared k-point (another spin channel), layout unchanged
+    void set_d_blocks(const double* dblk);
     template <typename R> int sticks_chunk(int nvec) const;
 
     // H|psi> on device vectors in precision R (the solver's building block)

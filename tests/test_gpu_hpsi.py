@@ -147,3 +147,21 @@ def test_host_buffer_path_matches_device_path(cuda_device, nvec):
         assert _rel(host, dev) < tol
     ref = ohpsi.apply_h(psi, sy.kpoints[0], sy.v_r, sy.cell.grid)
     assert _rel(ap.apply_batch_host(psi, nvec, FP64), ref) < FP64_TOL
+
+
+def test_spin_channel_d_blocks(cuda_device):
+    # set_spin_channel: the other channel's D blocks replace the prepared ones, and H|psi>
+    # is then the oracle's with those blocks (the projectors stay on the device)
+    import dataclasses
+    sy = synthetic.small_system(nbands=5, grid=(16, 16, 16), a=8.0, ecut=10.0, natoms=3)
+    kp = sy.kpoints[0]
+    ap = _applicator(sy)
+    rng = np.random.default_rng(4)
+    psi = rng.standard_normal((kp.npw, 6)) + 1j * rng.standard_normal((kp.npw, 6))
+    d_down = kp.d_blocks * 0.5 + rng.uniform(-0.1, 0.1, size=kp.d_blocks.shape) * (kp.d_blocks != 0)
+    ap.set_d_blocks(d_down)
+    kp_down = dataclasses.replace(kp, d_blocks=d_down)
+    for precision, tol in ((FP64, FP64_TOL), (MIXED, FP32_TOL)):
+        assert _rel(_run(ap, psi, precision), ohpsi.apply_h(psi, kp_down, sy.v_r, sy.cell.grid)) < tol
+    ap.set_d_blocks(kp.d_blocks)
+    assert _rel(_run(ap, psi), ohpsi.apply_h(psi, kp, sy.v_r, sy.cell.grid)) < FP64_TOL
