@@ -305,6 +305,28 @@ int q3b_server_wait(q3b_server* server, int id, q3b_cplx128* bands_out, double* 
 int q3b_hegv(q3b_context* ctx, int n, const q3b_cplx128* h_dev, const q3b_cplx128* s_dev, int ld,
              double* w_dev, q3b_cplx128* evec_dev);
 
+/* The same for the lowest nvec eigenpairs only (the Davidson's use,
+ * davidson.hpp:512-520): nvec eigenvalues to w_dev, evec_dev n x nvec (ld n). */
+int q3b_hegv_lowest(q3b_context* ctx, int n, const q3b_cplx128* h_dev, const q3b_cplx128* s_dev, int ld,
+                    int nvec, double* w_dev, q3b_cplx128* evec_dev);
+
+/* Many small problems in one launch, one thread block each (no counterpart in
+ * the reference, which solves one subspace at a time).  Problem i is
+ * H_i c = eps S_i c of order n[i] <= 128 with leading dimension ld[i], its
+ * lowest nvec[i] eigenpairs into w_dev[i] and evec_dev[i] (ld n[i]); the
+ * arrays of pointers and sizes are host arrays of `count` entries.  info_host[i]
+ * gets 0 or n[i] + j (S_i not positive definite at order j, zhegv's info).
+ * Returns Q3B_ERR_INVALID when a problem does not fit one block. */
+int q3b_hegv_batched(q3b_context* ctx, int count, const int* n, const q3b_cplx128* const* h_dev,
+                     const q3b_cplx128* const* s_dev, const int* ld, const int* nvec, double* const* w_dev,
+                     q3b_cplx128* const* evec_dev, int* info_host);
+
+/* Largest order the subspace eigensolver solves in one thread block (the
+ * others take the multi-kernel path); 0 sends every order to the multi-kernel
+ * path.  Process-wide; returns the previous value.  Default 56, below which the
+ * one-block solve is the faster of the two on a B200. */
+int q3b_set_block_eigensolver_order(int max_order);
+
 /* Counters of the context's CUDA-graph replays of the dense eigensolver: graphs
  * captured and replays served (either pointer may be NULL).  The launch
  * sequence of q3b_hegv and of the Davidson subspace solves of order >= 256 is

@@ -344,6 +344,69 @@ int q3b_davidson_solve(q3b_context* ctx, q3b_cplx128* bands, double* eig, int nb
     });
 }
 
+int q3b_hegv_lowest(q3b_context* ctx, int n, const q3b_cplx128* h, const q3b_cplx128* s, int ld, int nvec,
+                    double* w, q3b_cplx128* evec) {
+    return guarded(ctx, [&](Context& c) {
+        if (n < 0 || ld < n || nvec < 1 || nvec > n || (n > 0 && (!h || !s || !w || !evec)))
+            throw q3b::Status(Q3B_ERR_INVALID, "bad hegv arguments");
+        if (n == 0) return;
+        c.ws_dense.reserve(&c, q3b::dense::hegv_scratch_bytes(n));
+        q3b::dense::Scratch ws{c.ws_dense.as<char>(), c.ws_dense.bytes, 0};
+        q3b::GemmWorkspace g = c.gemm_ws(q3b::cgemm_workspace_bytes<double>(n, n, n));
+        const int info = q3b::dense::hegv(c.stream, n, reinterpret_cast<const double2*>(h),
+                                          reinterpret_cast<const double2*>(s), ld, w,
+                                          reinterpret_cast<double2*>(evec), nvec, ws, g, &c.hegv_graphs);
+        Q3B_CUDA(cudaStreamSynchronize(c.stream));
+        if (info != 0)
+            throw q3b::Status(Q3B_ERR_LINALG, "overlap matrix not positive definite (info " +
+                                                  std::to_string(info) + ")");
+    });
+}
+
+int q3b_hegv_batched(q3b_context* ctx, int count, const int* n, const q3b_cplx128* const* h,
+                     const q3b_cplx128* const* s, const int* ld, const int* nvec, double* const* w,
+                     q3b_cplx128* const* evec, int* info_host) {
+    return guarded(ctx, [&](Context& c) {
+        if (count < 0 || (count > 0 && (!n || !h || !s || !ld || !nvec || !w || !evec || !info_host)))
+            throw q3b::Status(Q3B_ERR_INVALID, "bad batched hegv arguments");
+        if (count == 0) return;
+        std::vector<q3b::dense::BlockProblem> probs(count);
+        size_t work = 0, smem = 0;
+        for (int i = 0; i < count; ++i) {
+            if (!q3b::dense::hegv_block_fits(n[i], nvec[i]) || ld[i] < n[i] || !h[i] || !s[i] || !w[i] || !evec[i])
+                throw q3b::Status(Q3B_ERR_INVALID, "batched hegv: problem " + std::to_string(i) +
+                                                       " does not fit one block");
+            work += (q3b::dense::hegv_block_work_elems(n[i]) + 16) & ~size_t(15);
+            smem = std::max(smem, q3b::dense::hegv_block_smem(n[i], nvec[i]));
+        }
+        // scratch: the problems' work areas, their status words and the descriptors
+        const size_t desc_off = work * sizeof(double2);
+        const size_t info_off = (desc_off + count * sizeof(q3b::dense::BlockProblem) + 255) & ~size_t(255);
+        c.ws_dense.reserve(&c, info_off + count * sizeof(int));
+        char* base = c.ws_dense.as<char>();
+        double2* wk = reinterpret_cast<double2*>(base);
+        int* info = reinterpret_cast<int*>(base + info_off);
+        for (int i = 0; i < count; ++i) {
+            probs[i] = q3b::dense::BlockProblem{n[i], ld[i], nvec[i], reinterpret_cast<const double2*>(h[i]),
+                                                reinterpret_cast<const double2*>(s[i]), w[i],
+                                                reinterpret_cast<double2*>(evec[i]), wk, info + i};
+            wk += (q3b::dense::hegv_block_work_elems(n[i]) + 16) & ~size_t(15);
+        }
+        auto* dev_probs = reinterpret_cast<q3b::dense::BlockProblem*>(base + desc_off);
+        Q3B_CUDA(cudaMemcpyAsync(dev_probs, probs.data(), count * sizeof(q3b::dense::BlockProblem),
+                                 cudaMemcpyHostToDevice, c.stream));
+        q3b::dense::hegv_block_many(c.stream, dev_probs, count, smem);
+        Q3B_CUDA(cudaMemcpyAsync(info_host, info, count * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+        Q3B_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int q3b_set_block_eigensolver_order(int max_order) {
+    const int prev = q3b::dense::block_max_order();
+    q3b::dense::set_block_max_order(max_order);
+    return prev;
+}
+
 int q3b_hegv(q3b_context* ctx, int n, const q3b_cplx128* h, const q3b_cplx128* s, int ld, double* w,
              q3b_cplx128* evec) {
     return guarded(ctx, [&](Context& c) {

@@ -225,7 +225,7 @@ template <typename R> class Davidson {
                        + 2 * mm * sizeof(double2)                                 // Hs, Ss
                        + 3 * mm * sizeof(double2)                                 // evec, gram64, uinv64
                        + 5 * mm * sizeof(T)                                       // evecR, cpack, cneg, coef, uinvR
-                       + 4 * (size_t)maxn_ * sizeof(double) + (size_t)maxn_ * sizeof(int) +
+                       + 4 * (size_t)maxn_ * sizeof(double) + (size_t)maxn_ * sizeof(int) + 512 +
                        (size_t)npw_ * sizeof(double) + 32 * 256;
         mem.reserve(&c, bytes);
         Carve cv{mem.as<char>()};
@@ -253,6 +253,7 @@ template <typename R> class Davidson {
         eps_ = cv.take<double>(maxn_);
         norms_ = cv.take<double>(maxn_);
         idx_ = cv.take<int>(maxn_);
+        dinfo_ = cv.take<int>(4);
         ke_ = c.kp.ke64.as<double>();
         dmem.reserve(&c, dense::hegv_scratch_bytes(maxn_) + dense::potrf_scratch_bytes(maxn_));
         dscratch_.base = dmem.as<char>();
@@ -303,12 +304,8 @@ template <typename R> class Davidson {
         // Cholesky QR, the Gram matrix T^H S T and its factor in FP64
         inner(ncand, ncand, Tc, STc, coef_, ncand);
         widen(ncand, ncand, coef_, ncand, gram_, ncand);
-        dscratch_.used = 0;
-        const int info = dense::potrf(st_, ncand, gram_, ncand, dscratch_);
+        const int info = cholesky_inverse(ncand);
         if (info == 0) {
-            // the same scratch still holds the diagonal-block inverses potrf left
-            dscratch_.used = 0;
-            dense::trtri_after_potrf(st_, ncand, gram_, ncand, uinv_, dscratch_);
             const T* U = narrowed(ncand, ncand, uinv_, ncand, uinvR_);
             gemm(false, npw_, ncand, ncand, one(), Tc, npw_, U, ncand, zero(), tmp_, npw_);
             Q3B_CUDA(cudaMemcpyAsync(Tc, tmp_, (size_t)npw_ * ncand * sizeof(T), cudaMemcpyDeviceToDevice, st_));
@@ -346,6 +343,25 @@ template <typename R> class Davidson {
             }
         }
         return accepted;
+    }
+
+    // gram_ = U^H U and uinv_ = U^{-1} (ld n); LAPACK's potrf info (0: positive definite)
+    int cholesky_inverse(int n) {
+        if (n <= dense::block_max_order() && dense::chol_inverse_block_fits(n)) {
+            dense::chol_inverse_block(st_, n, gram_, n, uinv_, dinfo_);
+            int* h = static_cast<int*>(host_readback(sizeof(int)));
+            Q3B_CUDA(cudaMemcpyAsync(h, dinfo_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+            Q3B_CUDA(cudaStreamSynchronize(st_));
+            return h[0];
+        }
+        dscratch_.used = 0;
+        const int info = dense::potrf(st_, n, gram_, n, dscratch_);
+        if (info == 0) {
+            // the same scratch still holds the diagonal-block inverses potrf left
+            dscratch_.used = 0;
+            dense::trtri_after_potrf(st_, n, gram_, n, uinv_, dscratch_);
+        }
+        return info;
     }
 
     // ------------------------------------ update_subspace_matrices (serial.hpp:555-678)
@@ -762,6 +778,7 @@ template <typename R> class Davidson {
     double2 *Hs_, *Ss_, *evec_, *gram_, *uinv_;
     double *w_, *eps_, *norms_;
     int* idx_;
+    int* dinfo_ = nullptr;  // status word of the block Cholesky
     const double* ke_;
     dense::Scratch dscratch_;
     std::vector<double> whost_;

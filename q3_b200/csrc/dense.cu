@@ -17,12 +17,14 @@
 //         clusters of close eigenvalues, then Z = Q (phase * Y) by GEMM.
 #include <cstring>
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <mutex>
 #include <vector>
 
 #include "context.cuh"
 #include "dense.cuh"
+#include "tridiag.cuh"
 #include "q3b.h"
 
 namespace q3b {
@@ -560,47 +562,6 @@ __global__ void apply_phase(int n, int nvec, const double2* phase, const double*
     }
 }
 
-// numbers of eigenvalues of the real tridiagonal (d, e2) below x[0..S).  The
-// count is the number of sign changes along p_0 = 1, p_1, ..., p_n with
-// p_k = (d_k - x) p_{k-1} - e2_{k-1} p_{k-2} (the leading principal minors of
-// T - x I); the ratio p_k / p_{k-1} is the pivot of the LDL^T form, and a
-// ratio below pivmin in magnitude is replaced by -pivmin, as in the LDL^T
-// count.  No division: each step rescales the pair by the power of two of
-// p_{k-1} (exact), which keeps both in range, so the dependent chain per step
-// is one FMA, a select and a multiply.  S independent recurrences interleave.
-__device__ __forceinline__ double pow2_inverse_exponent(double p) {
-    // the exponent field sits in bits 20..30 of the high word: 32-bit integer
-    // work only
-    const int e = (__double2hiint(p) >> 20) & 0x7ff;
-    return __hiloint2double((2046 - e) << 20, 0);
-}
-
-template <int S>
-__device__ __forceinline__ void sturm_counts(int n, const double* d, const double* e2, const double* x,
-                                             double pivmin, int* c) {
-    double p[S], pm[S];
-#pragma unroll
-    for (int s = 0; s < S; ++s) {
-        pm[s] = 1.0;
-        p[s] = d[0] - x[s];
-        if (fabs(p[s]) < pivmin) p[s] = -pivmin;
-        c[s] = p[s] < 0.0;
-    }
-#pragma unroll 4
-    for (int k = 1; k < n; ++k) {
-        const double dk = d[k], ek = e2[k - 1];
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const double sc = pow2_inverse_exponent(p[s]);
-            double q = fma(dk - x[s], p[s], -ek * pm[s]);
-            if (fabs(q) < pivmin * fabs(p[s])) q = -pivmin * p[s];
-            c[s] += (q < 0.0) != (p[s] < 0.0);
-            pm[s] = p[s] * sc;
-            p[s] = q * sc;
-        }
-    }
-}
-
 // one warp per eigenvalue (the lowest nw): multisection of [lo, hi] on Sturm
 // counts at 32 x kShifts interior points per round (the interval shrinks
 // 65-fold).  The block stages d and e^2 in shared memory when they fit
@@ -742,10 +703,6 @@ __global__ void tridiag_invit(int n, const double* d, const double* ea, const do
 // step of each sweep is a few shared-memory accesses and fused multiply-adds.
 // blockDim.x threads (one per eigenvalue) share the block's shared memory:
 // 41 bytes per thread and row.
-__device__ __forceinline__ double clamp_tiny(double x, double tiny) {
-    return fabs(x) < tiny ? (x < 0.0 ? -tiny : tiny) : x;
-}
-
 __global__ void tridiag_invit_smem(int n, const double* d, const double* ea, const double* w,
                                    const double* bounds, int nvec, double* Y) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1148,9 +1105,31 @@ cudaGraphExec_t HegvGraphs::capture(cudaStream_t st, void (*issue)(void*), void*
     return exec;
 }
 
+namespace {
+std::atomic<int> g_block_max_order{kBlockOrderDefault};
+}  // namespace
+
+void set_block_max_order(int n) { g_block_max_order.store(n < 0 ? 0 : n); }
+int block_max_order() { return g_block_max_order.load(); }
+
 int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, double* w, double2* Z,
          int nvec, Scratch& ws, const GemmWorkspace& gws, HegvGraphs* graphs, double* w_host) {
     if (n <= 0) return 0;
+    const int nv = nvec > 0 ? nvec : n;
+    if (n <= block_max_order() && hegv_block_fits(n, nv)) {
+        // one block: a single launch and one synchronisation (dense_block.cu)
+        double2* work = ws.take<double2>(hegv_block_work_elems(n));
+        int* info = ws.take<int>(1);
+        hegv_block(st, BlockProblem{n, ld, nv, H, S, w, Z, work, info});
+        char* hb = static_cast<char*>(host_readback(sizeof(double) + (w_host ? nv * sizeof(double) : 0)));
+        int* flag = reinterpret_cast<int*>(hb);
+        double* wb = reinterpret_cast<double*>(hb + sizeof(double));
+        Q3B_CUDA(cudaMemcpyAsync(flag, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+        if (w_host) Q3B_CUDA(cudaMemcpyAsync(wb, w, nv * sizeof(double), cudaMemcpyDeviceToHost, st));
+        Q3B_CUDA(cudaStreamSynchronize(st));
+        if (w_host) std::memcpy(w_host, wb, nv * sizeof(double));
+        return flag[0];
+    }
     const size_t used0 = ws.used;
     const size_t nn = (size_t)n * n;
     // every slice first, in a fixed order: the same pointers on every call

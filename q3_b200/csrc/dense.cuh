@@ -127,6 +127,41 @@ int hegv(cudaStream_t st, int n, const double2* H, const double2* S, int ld, dou
          int nvec, Scratch& ws, const GemmWorkspace& gws, HegvGraphs* graphs = nullptr,
          double* w_host = nullptr);
 
+// One problem of the block eigensolver (dense_block.cu): H c = w S c of order
+// n <= 128 (upper triangles, ld ld), the lowest nvec eigenpairs into w and Z
+// (n x nvec, ld n), status into *info (0, or n + j as hegv); `work` holds
+// hegv_block_work_elems(n) complex values.  Device pointers.
+struct BlockProblem {
+    int n, ld, nvec;
+    const double2* H;
+    const double2* S;
+    double* w;
+    double2* Z;
+    double2* work;
+    int* info;
+};
+size_t hegv_block_smem(int n, int nvec);
+// whether a block holds a problem of this order and vector count
+bool hegv_block_fits(int n, int nvec);
+size_t hegv_block_work_elems(int n);
+// one problem, one block of 512 threads; no host synchronisation
+void hegv_block(cudaStream_t st, const BlockProblem& p);
+// `count` problems (descriptors in device memory, each checked by
+// hegv_block_fits), one block each; smem = the largest hegv_block_smem of them
+void hegv_block_many(cudaStream_t st, const BlockProblem* problems_dev, int count, size_t smem);
+
+// G = U^H U (upper triangle of G, ld ldg) and Uinv = U^{-1} (n x n, ld n, zero
+// below the diagonal) in one block; *info = 0, or k+1 when the leading minor of
+// order k+1 is not positive definite (potrf's info).  No host synchronisation.
+bool chol_inverse_block_fits(int n);
+void chol_inverse_block(cudaStream_t st, int n, const double2* G, int ldg, double2* Uinv, int* info);
+
+// hegv runs problems up to this order on one block (when hegv_block_fits);
+// 0 keeps every order on the multi-kernel path
+constexpr int kBlockOrderDefault = 56;
+void set_block_max_order(int n);
+int block_max_order();
+
 // Whether hegv/heev take a problem of order n on the current device (the
 // tridiagonalisation keeps its blocks' columns in shared memory).
 bool order_supported(int n);

@@ -121,3 +121,55 @@ def hegv(applicator, h: np.ndarray, s: np.ndarray):
         rc = applicator.lib.q3b_hegv(applicator.h, n, H.data_ptr(), S.data_ptr(), n, w.data_ptr(), Z.data_ptr())
     check(applicator.h, rc)
     return w.cpu().numpy(), Z.cpu().numpy().T
+
+
+def hegv_lowest(applicator, h: np.ndarray, s: np.ndarray, nvec: int):
+    """The lowest nvec eigenpairs of H c = w S c on the GPU (upper triangles used)."""
+    import torch
+    n = h.shape[0]
+    dev = torch.device("cuda", applicator.ctx.device)
+    H = torch.from_numpy(np.ascontiguousarray(np.asarray(h, np.complex128).T)).to(dev)
+    S = torch.from_numpy(np.ascontiguousarray(np.asarray(s, np.complex128).T)).to(dev)
+    w = torch.empty(nvec, dtype=torch.float64, device=dev)
+    Z = torch.empty(nvec, n, dtype=torch.complex128, device=dev)
+    with applicator.ctx.ordered_with_torch():
+        rc = applicator.lib.q3b_hegv_lowest(applicator.h, n, H.data_ptr(), S.data_ptr(), n, int(nvec),
+                                            w.data_ptr(), Z.data_ptr())
+    check(applicator.h, rc)
+    return w.cpu().numpy(), Z.cpu().numpy().T
+
+
+def hegv_batched(applicator, problems):
+    """Many small generalized problems in one launch: `problems` is a list of (h, s, nvec);
+    returns a list of (w, Z, info) with info 0 or n + j (S not positive definite)."""
+    import torch
+    dev = torch.device("cuda", applicator.ctx.device)
+    count = len(problems)
+    keep, ns, lds, nvs, hp, sp, wp, zp = [], [], [], [], [], [], [], []
+    for h, s, nvec in problems:
+        n = h.shape[0]
+        H = torch.from_numpy(np.ascontiguousarray(np.asarray(h, np.complex128).T)).to(dev)
+        S = torch.from_numpy(np.ascontiguousarray(np.asarray(s, np.complex128).T)).to(dev)
+        w = torch.empty(nvec, dtype=torch.float64, device=dev)
+        Z = torch.empty(nvec, n, dtype=torch.complex128, device=dev)
+        keep.append((H, S, w, Z))
+        ns.append(n)
+        lds.append(n)
+        nvs.append(int(nvec))
+        hp.append(H.data_ptr())
+        sp.append(S.data_ptr())
+        wp.append(w.data_ptr())
+        zp.append(Z.data_ptr())
+    I = C.c_int * count
+    V = C.c_void_p * count
+    info = I()
+    with applicator.ctx.ordered_with_torch():
+        rc = applicator.lib.q3b_hegv_batched(applicator.h, count, I(*ns), V(*hp), V(*sp), I(*lds), I(*nvs),
+                                             V(*wp), V(*zp), info)
+    check(applicator.h, rc)
+    return [(w.cpu().numpy(), Z.cpu().numpy().T, int(info[i])) for i, (_H, _S, w, Z) in enumerate(keep)]
+
+
+def set_block_eigensolver_order(max_order: int) -> int:
+    """Largest subspace order solved in one thread block (0: none); returns the previous."""
+    return int(_lib.load().q3b_set_block_eigensolver_order(int(max_order)))
