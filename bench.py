@@ -65,6 +65,9 @@ def parse():
                          "density of --density-bands bands of the bench cell (density), run the "
                          "converged precision study (precision) or the config-4 request stream "
                          "alone (serving), and exit; prints no bench line")
+    ap.add_argument("--local-kernel", type=int, default=0,
+                    help="plane kernel of the bench cell (threads > 0 or -lanes for the register "
+                         "kernel; 0: the autotuner's choice)")
     ap.add_argument("--density-bands", type=int, default=39,
                     help="bands for --probe density (39: one stick chunk of the 80^3 cell in FP64)")
     ap.add_argument("--hegv-orders", default="16,32,64,96,128,192,256,384,512",
@@ -683,6 +686,28 @@ def request_stream(specs, ex, workers: int):
         yield sy
 
 
+def tight_check(spec, fp64_res, mixed_res, diff):
+    """One request solved again in FP64 to an eigenvalue change of 1e-12 Ry (up to 2000
+    iterations), and the served FP64 and mixed eigenvalues' errors against it (Ha)."""
+    from q3_b200 import synthetic
+    from q3_b200._lib import FP64
+    from q3_b200.applicator import PlanewaveHamiltonianApplicator
+    from q3_b200.davidson import PlanewaveDavidsonDiagonalizer
+    sy = synthetic.build_request(spec)
+    ap = PlanewaveHamiltonianApplicator()
+    ap.update_potential(sy.v_r, sy.cell.grid)
+    ap.prepare_system_kpoint(sy)
+    dv = PlanewaveDavidsonDiagonalizer(ap, FP64)
+    dv.set_tolerance(1e-12)
+    dv.set_maximum_iterations(2000)
+    r = dv.solve(sy.psi0[0], sy.nbands)
+    ap.ctx.close()
+    return {"npw": int(sy.kpoints[0].npw), "bands": int(sy.nbands), "mixed_vs_fp64_ha": diff / 2.0,
+            "fp64_vs_tight_ha": float(np.max(np.abs(fp64_res.eigenvalues - r.eigenvalues))) / 2.0,
+            "mixed_vs_tight_ha": float(np.max(np.abs(mixed_res.eigenvalues - r.eigenvalues))) / 2.0,
+            "tight_iterations": int(r.iterations), "tight_unconverged": int(r.unconverged)}
+
+
 def config4_section(args):
     from q3_b200 import synthetic
     from q3_b200._lib import FP64, MIXED
@@ -707,8 +732,12 @@ def config4_section(args):
         srv.close()
         cap_res[name] = o.pop("results")
         cap[name] = o
-    both = [(a, g) for a, g in zip(cap_res["fp64"], cap_res["mixed"]) if not a.unconverged and not g.unconverged]
-    err4 = max(float(np.max(np.abs(a.eigenvalues - g.eigenvalues))) for a, g in both) if both else float("nan")
+    both = [(i, a, g) for i, (a, g) in enumerate(zip(cap_res["fp64"], cap_res["mixed"]))
+            if not a.unconverged and not g.unconverged]
+    diffs = sorted((float(np.max(np.abs(a.eigenvalues - g.eigenvalues))), i, a, g) for i, a, g in both)
+    err4 = diffs[-1][0] if diffs else float("nan")
+    # the requests where the two differ most, against an FP64 solve to 1e-12 Ry
+    tight = [tight_check(specs[i], a, g, d) for d, i, a, g in diffs[-3:]]
     rate = args.serving_rate if args.serving_rate > 0 else 0.8 * cap["fp64"]["solves_per_s"]
     streams = {}
     for name, prec in (("fp64", FP64), ("mixed", MIXED)):
@@ -728,6 +757,7 @@ def config4_section(args):
             "capacity": {"rule": f"closed loop, {WINDOW} requests in the server", **cap},
             "capacity_speedup": cap["mixed"]["solves_per_s"] / cap["fp64"]["solves_per_s"],
             "mixed_vs_fp64_max_eig_err_ha": err4 / 2.0,
+            "largest_differences_vs_tight_fp64": tight,
             "rate_hz": rate, "rate_rule": "0.8 x FP64 capacity", "poisson_streams": streams,
             "p50_p99_speedup": {k: streams["fp64"]["median_of_streams"][k] / streams["mixed"]["median_of_streams"][k]
                                 for k in ("p50_ms", "p99_ms")}}
@@ -758,6 +788,11 @@ def run_q3b(args):
     ap = PlanewaveHamiltonianApplicator(device=local)
     ap.update_potential(sy.v_r, sy.cell.grid)
     ap.prepare_system_kpoint(sy)
+    if args.local_kernel:
+        # a fixed plane kernel for both precisions (an ncu run then launches the same
+        # kernels as the plain run, whose tuner picks by timing)
+        for prec in (MIXED, FP64):
+            ap.set_local_kernel(args.local_kernel, prec)
     lib, h = ap.lib, ap.h
     stream = torch.cuda.ExternalStream(ap.ctx.stream, device=dev)
 
@@ -1050,6 +1085,8 @@ def run_probe(args):
     x = torch.from_numpy(np.ascontiguousarray(sy.psi0[0].T)).to("cuda")
     y = torch.empty_like(x)
     prec = MIXED if args.probe == "mixed" else FP64
+    if args.local_kernel:
+        ap.set_local_kernel(args.local_kernel, prec)
     for _ in range(3):
         ap.apply_batch(x, y, sy.nbands, prec)
     torch.cuda.synchronize()
