@@ -190,6 +190,22 @@ def kernel_bytes(kp, grid, nsticks, nvec, c, r):
     }
 
 
+def plane_flops(kp, grid, nvec):
+    """Flops of the plane pass for nvec bands: per (band, w3) plane the backward and forward
+    transforms of the rows holding sticks (length n2) and of all columns (length n1), at
+    5 n log2 n each, and the V(r) product (2 flops a complex point)."""
+    n1, n2, n3 = grid
+    rows = len(np.unique(np.asarray(kp.g_to_grid) // (n2 * n3)))
+    line = lambda n: 5.0 * n * np.log2(n)
+    per_plane = 2 * rows * line(n2) + 2 * n2 * line(n1) + 2.0 * n1 * n2
+    return float(nvec * n3 * per_plane)
+
+
+def device_sms_of(dev):
+    import torch
+    return int(torch.cuda.get_device_properties(dev).multi_processor_count)
+
+
 def kernel_flops(kp, nvec):
     return {"projector_overlap": 8.0 * kp.npw * kp.nproj * nvec,
             "projector_accumulate": 8.0 * kp.npw * kp.nproj * nvec}
@@ -949,6 +965,15 @@ def run_q3b(args):
                 "frac": achieved / hbm, "peak_note": f"{peak_kind} copy bandwidth",
                 "algorithmic_bytes_per_launch": per_launch, "traffic": traffic,
                 "launches": n_dom, "ms": ms_dom}
+        if name == "planes":
+            # the same kernel against the FP32 pipe: its transform flops (5 n log2 n per
+            # length-n line, the usual count) and the V product, at the nominal FMA rate
+            fl = plane_flops(kp, sy.cell.grid, nb)
+            clk = clocks.summary().get("sm_mhz") or 1965.0
+            peak32 = device_sms_of(dev) * 128 * 2 * clk * 1e6 / 1e12
+            roof["fp32_pipe"] = {"flops_per_step": fl, "achieved_tflops": fl / (ms_dom * 1e-3) / 1e12,
+                                 "peak_tflops": peak32, "frac": fl / (ms_dom * 1e-3) / 1e12 / peak32,
+                                 "peak_note": "nominal FP32 FMA rate: SMs x 128 lanes x 2 x the median SM clock"}
 
     cpu = None
     if world == 1 and not args.no_cpu:
