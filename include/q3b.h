@@ -294,6 +294,17 @@ int q3b_server_poll(q3b_server* server, int id);
 int q3b_server_wait(q3b_server* server, int id, q3b_cplx128* bands_out, double* eigenvalues_out,
                     q3b_davidson_stats* stats, q3b_request_times* times);
 
+/* Batch the running solves' subspace eigensolves (enable != 0): each Davidson
+ * iteration's generalized eigenproblem of order <= about 110 is solved in one
+ * launch together with those of the other workers that reach the same step,
+ * one thread block per problem; a batch waits up to wait_us microseconds
+ * (0: 200) for workers busy elsewhere.  Only while the server is idle
+ * (Q3B_ERR_STATE otherwise).  A problem that fits one block is solved the same
+ * way whatever batch it joins, so results do not depend on the mix. */
+int q3b_server_set_batching(q3b_server* server, int enable, int wait_us);
+/* batches launched and problems they solved so far */
+int q3b_server_batch_stats(q3b_server* server, long* batches, long* problems);
+
 /* ---- dense FP64 subspace kernels (PlanewaveSubspaceManager pieces) ---------- */
 
 /* diagonalize_subspace (subspace_manager/init.hpp:82; subspace/serial.hpp:18-151):

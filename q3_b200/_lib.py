@@ -122,6 +122,8 @@ SIGNATURES = {
     "q3b_set_overlap_blocks": (_i, [_vp, _vp]),
     "q3b_set_d_blocks": (_i, [_vp, _vp]),
     "q3b_hegv_lowest": (_i, [_vp, _i, _vp, _vp, _i, _i, _vp, _vp]),
+    "q3b_server_set_batching": (_i, [_vp, _i, _i]),
+    "q3b_server_batch_stats": (_i, [_vp, _vp, _vp]),
     "q3b_hegv_batched": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "q3b_set_block_eigensolver_order": (_i, [_i]),
     "q3b_apply_s": (_i, [_vp, _vp, _vp, _i, _i]),

@@ -22,6 +22,7 @@ struct Status : std::runtime_error {
 };
 
 class Context;
+class EigenBatcher;
 
 // A device allocation charged to its context's HBM budget.
 struct DevBuf {
@@ -85,6 +86,9 @@ class Context {
     DevBuf ws_mixed;  // FP64 bands of a mixed solve between its phases (buffer bands included)
     // replays of the dense eigensolver's launch sequence (one per context)
     dense::HegvGraphs hegv_graphs;
+    // when set (a serving worker's context), the Davidson's subspace eigensolves
+    // that fit one block go through this batcher, shared with the other workers
+    EigenBatcher* batcher = nullptr;
     // charge density: per-group partial sums and the band weights
     DevBuf ws_density;
     // starting-subspace rotation: chi and H chi of the last q3b_start_apply

@@ -23,6 +23,7 @@
 #include <numeric>
 #include <vector>
 
+#include "batcher.cuh"
 #include "davidson.cuh"
 #include "dense.cuh"
 #include "gamma.cuh"
@@ -388,6 +389,16 @@ template <typename R> class Davidson {
     int diagonalize(int n, const double2* H, const double2* S, int ld, bool publish = true) {
         dscratch_.used = 0;
         const int nvec = std::min(nb_, n);
+        if (c_.batcher && EigenBatcher::takes(n, nvec)) {
+            // in a batch with the other workers' solves (batcher.cuh)
+            double2* work = dscratch_.take<double2>(dense::hegv_block_work_elems(n));
+            int* info = dscratch_.take<int>(1);
+            wread_.assign(n, 0.0);
+            const int st = c_.batcher->solve(dense::BlockProblem{n, ld, nvec, H, S, w_, evec_, work, info}, st_,
+                                              wread_.data());
+            if (st == 0 && publish) whost_.assign(wread_.begin(), wread_.begin() + nvec);
+            return st;
+        }
         GemmWorkspace gws = c_.gemm_ws(cgemm_workspace_bytes<double>(n, n, n));
         // the lowest nvec eigenvalues come back in the solve's own status read
         wread_.assign(n, 0.0);

@@ -20,6 +20,7 @@
 #include <thread>
 #include <vector>
 
+#include "batcher.cuh"
 #include "context.cuh"
 #include "davidson.cuh"
 #include "dense.cuh"
@@ -118,6 +119,21 @@ class Server {
         return j ? (j->done ? 1 : 0) : -1;
     }
 
+    // Batch the workers' subspace eigensolves (batcher.cuh); only while no request is
+    // queued or running.  wait_us: how long a batch waits for workers busy elsewhere.
+    void set_batching(bool on, int wait_us) {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (running_ > 0 || !queue_.empty())
+            throw Status(Q3B_ERR_STATE, "batching can only change while the server is idle");
+        batcher_.reset(on ? new EigenBatcher(device_, wait_us) : nullptr);
+        for (auto& c : ctxs_) c->impl.batcher = batcher_.get();
+    }
+    void batch_stats(long* batches, long* problems) {
+        std::lock_guard<std::mutex> lk(mu_);
+        *batches = batcher_ ? batcher_->batches() : 0;
+        *problems = batcher_ ? batcher_->problems() : 0;
+    }
+
     std::unique_ptr<Job> wait(int id) {
         std::unique_lock<std::mutex> lk(mu_);
         Job* j = find(id);
@@ -137,6 +153,7 @@ class Server {
         cudaSetDevice(device_);
         while (true) {
             Job* j = nullptr;
+            EigenBatcher* batcher = nullptr;
             {
                 std::unique_lock<std::mutex> lk(mu_);
                 cv_work_.wait(lk, [&] {
@@ -149,10 +166,13 @@ class Server {
                 queue_.erase(it);
                 in_use_ += j->est;
                 ++running_;
+                batcher = batcher_.get();
+                if (batcher) batcher->join();
             }
             j->t_start = now_s();
             solve(ctx, *j);
             j->t_end = now_s();
+            if (batcher) batcher->leave();
             {
                 std::lock_guard<std::mutex> lk(mu_);
                 in_use_ -= j->est;
@@ -211,6 +231,7 @@ class Server {
     std::condition_variable cv_work_, cv_done_;
     std::deque<Job*> queue_;
     std::map<int, std::unique_ptr<Job>> jobs_;
+    std::unique_ptr<EigenBatcher> batcher_;
     std::vector<std::unique_ptr<q3b_context>> ctxs_;
     std::vector<std::thread> threads_;
 };
@@ -240,6 +261,26 @@ int q3b_server_create(int device, size_t hbm_budget_bytes, int workers, q3b_serv
     } catch (const std::exception&) {
         return Q3B_ERR_CUDA;
     }
+}
+
+int q3b_server_set_batching(q3b_server* s, int enable, int wait_us) {
+    if (!s) return Q3B_ERR_INVALID;
+    try {
+        s->impl->set_batching(enable != 0, wait_us > 0 ? wait_us : 200);
+        return Q3B_OK;
+    } catch (const q3b::Status& e) {
+        s->err = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        s->err = e.what();
+        return Q3B_ERR_CUDA;
+    }
+}
+
+int q3b_server_batch_stats(q3b_server* s, long* batches, long* problems) {
+    if (!s || !batches || !problems) return Q3B_ERR_INVALID;
+    s->impl->batch_stats(batches, problems);
+    return Q3B_OK;
 }
 
 int q3b_server_destroy(q3b_server* s) {

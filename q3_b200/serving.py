@@ -34,7 +34,10 @@ class Served:
 
 
 class BandSolveServer:
-    def __init__(self, device: int = 0, hbm_budget: int = 0, workers: int = 4):
+    def __init__(self, device: int = 0, hbm_budget: int = 0, workers: int = 4, batching: bool = False,
+                 batch_wait_us: int = 200):
+        """batching: solve the workers' subspace eigenproblems in shared launches (one block
+        each) as they reach that step together (q3b_server_set_batching)."""
         self.lib = _lib.load()
         h = C.c_void_p()
         rc = self.lib.q3b_server_create(int(device), int(hbm_budget), int(workers), C.byref(h))
@@ -42,6 +45,14 @@ class BandSolveServer:
             raise _lib.Q3BError(rc, "cannot create a server")
         self.h = h.value
         self._shape: Dict[int, tuple] = {}
+        if batching:
+            self._check(self.lib.q3b_server_set_batching(self.h, 1, int(batch_wait_us)))
+
+    def batch_stats(self):
+        """(batches launched, problems solved in them)."""
+        b, p = C.c_long(), C.c_long()
+        self._check(self.lib.q3b_server_batch_stats(self.h, C.byref(b), C.byref(p)))
+        return b.value, p.value
 
     def close(self) -> None:
         if getattr(self, "h", None):

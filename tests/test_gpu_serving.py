@@ -73,3 +73,33 @@ def test_server_matches_direct_solve(cuda_device):
     got = srv.wait(srv.submit(sy, tolerance=1e-9, max_iterations=100))
     srv.close()
     assert np.max(np.abs(got.eigenvalues - direct.eigenvalues)) < 1e-12
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED], ids=["fp64", "mixed"])
+def test_batched_eigensolves(cuda_device, precision):
+    # workers share their subspace eigensolves' launches: the results are the same alone
+    # and in the mix, batches hold several problems, and the solves agree with an
+    # unbatched server to rounding (the one-block eigensolver in place of the
+    # multi-kernel one above order 56)
+    from q3_b200.serving import BandSolveServer
+    sy2 = synthetic.config(2)
+    systems = [(sy2, k) for k in range(8)] + [(s, 0) for s in _systems()[:3]]
+    kw = dict(tolerance=1e-9, max_iterations=200, precision=precision)
+    many = BandSolveServer(workers=8, batching=True)
+    ids = [many.submit(sy, k=k, **kw) for sy, k in systems]
+    mixed = [many.wait(i) for i in ids]
+    batches, problems = many.batch_stats()
+    many.close()
+    assert problems > batches > 0
+    one = BandSolveServer(workers=1, batching=True)
+    alone = [one.wait(one.submit(sy, k=k, **kw)) for sy, k in systems]
+    one.close()
+    plain = BandSolveServer(workers=4)
+    ids = [plain.submit(sy, k=k, **kw) for sy, k in systems]
+    ref = [plain.wait(i) for i in ids]
+    plain.close()
+    for a, m, r in zip(alone, mixed, ref):
+        assert m.unconverged == 0
+        assert np.max(np.abs(a.eigenvalues - m.eigenvalues)) < 1e-12
+        assert a.iterations == m.iterations
+        assert np.max(np.abs(m.eigenvalues - r.eigenvalues)) < (4e-8 if precision == MIXED else 1e-8)
