@@ -334,7 +334,7 @@ int q3b_hegv_batched(q3b_context* ctx, int count, const int* n, const q3b_cplx12
 
 /* Largest order the subspace eigensolver solves in one thread block (the
  * others take the multi-kernel path); 0 sends every order to the multi-kernel
- * path.  Process-wide; returns the previous value.  Default 56, below which the
+ * path.  Process-wide; returns the previous value.  Default 64, up to which the
  * one-block solve is the faster of the two on a B200. */
 int q3b_set_block_eigensolver_order(int max_order);
 

@@ -158,7 +158,7 @@ void chol_inverse_block(cudaStream_t st, int n, const double2* G, int ldg, doubl
 
 // hegv runs problems up to this order on one block (when hegv_block_fits);
 // 0 keeps every order on the multi-kernel path
-constexpr int kBlockOrderDefault = 56;
+constexpr int kBlockOrderDefault = 64;
 void set_block_max_order(int n);
 int block_max_order();
 

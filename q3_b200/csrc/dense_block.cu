@@ -88,10 +88,11 @@ __device__ __forceinline__ bool cholesky_in_smem(int n, int P, const double2* S,
         const double rs = 1.0 / sqrt(piv);
         for (int j = k + 1 + tid; j < n; j += kBT) A[k + (size_t)j * P] = rs * A[k + (size_t)j * P];
         __syncthreads();
-        const int m = n - k - 1;
-        for (int idx = tid; idx < m * m; idx += kBT) {
-            const int i = k + 1 + idx % m, j = k + 1 + idx / m;
-            if (i <= j) A[i + (size_t)j * P] = A[i + (size_t)j * P] - cmulc(A[k + (size_t)i * P], A[k + (size_t)j * P]);
+        // trailing update of the upper triangle: a warp per column j, lanes along rows i <= j
+        for (int j = k + 1 + (tid >> 5); j < n; j += kBW) {
+            const double2 ukj = A[k + (size_t)j * P];
+            double2* col = A + (size_t)j * P;
+            for (int i = k + 1 + (tid & 31); i <= j; i += 32) col[i] = col[i] - cmulc(A[k + (size_t)i * P], ukj);
         }
         if (tid == 0) A[k + (size_t)k * P] = mk(sqrt(piv), 0.0);
         __syncthreads();
@@ -101,22 +102,33 @@ __device__ __forceinline__ bool cholesky_in_smem(int n, int P, const double2* S,
     return true;
 }
 
-// U^{-1} (n x n, ld n, zero below the diagonal) into Uinv from the factor in A:
-// column c solves U x = e_c by back substitution, one warp per column, x
-// staged in the warp's xw
-__device__ __forceinline__ void inverse_to_global(int n, int P, const double2* A, const double* rdiag, double2* xw,
-                                                  double2* Uinv) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int c = warp; c < n; c += kBW) {
+// U^{-1} (n x n, ld n, zero below the diagonal) into Uinv from the factor in A.
+// Thread c solves U x = e_c by back substitution; x is kept transposed in row c
+// of A's lower triangle (x_r at A[c][r], r <= c), which no other column reads,
+// while every thread reads the strictly upper U.  Four accumulators shorten the
+// dependent FMA chain of each dot product.
+__device__ __forceinline__ void inverse_to_global(int n, int P, double2* A, const double* rdiag, double2* Uinv) {
+    const int c = threadIdx.x;
+    if (c < n) {
+        double2* xr = A + c;  // x_r at xr[r * P]
         for (int r = c; r >= 0; --r) {
-            double2 s = mk(0.0, 0.0);
-            for (int k = r + 1 + lane; k <= c; k += 32) cfma(s, A[r + (size_t)k * P], xw[k]);
-            s = wsum2(s);
-            if (lane == 0) xw[r] = rdiag[r] * mk(((r == c) ? 1.0 : 0.0) - s.x, -s.y);
-            __syncwarp();
+            double2 s0 = mk(0.0, 0.0), s1 = mk(0.0, 0.0), s2 = mk(0.0, 0.0), s3 = mk(0.0, 0.0);
+            int k = r + 1;
+            for (; k + 3 <= c; k += 4) {
+                cfma(s0, A[r + (size_t)k * P], xr[(size_t)k * P]);
+                cfma(s1, A[r + (size_t)(k + 1) * P], xr[(size_t)(k + 1) * P]);
+                cfma(s2, A[r + (size_t)(k + 2) * P], xr[(size_t)(k + 2) * P]);
+                cfma(s3, A[r + (size_t)(k + 3) * P], xr[(size_t)(k + 3) * P]);
+            }
+            for (; k <= c; ++k) cfma(s0, A[r + (size_t)k * P], xr[(size_t)k * P]);
+            const double2 sum = (s0 + s1) + (s2 + s3);
+            xr[(size_t)r * P] = rdiag[r] * mk(((r == c) ? 1.0 : 0.0) - sum.x, -sum.y);
         }
-        for (int r = lane; r < n; r += 32) Uinv[r + (size_t)c * n] = r <= c ? xw[r] : mk(0.0, 0.0);
-        __syncwarp();
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < n * n; idx += kBT) {
+        const int r = idx % n, col = idx / n;
+        Uinv[idx] = r <= col ? A[col + (size_t)r * P] : mk(0.0, 0.0);
     }
 }
 
@@ -126,6 +138,7 @@ __device__ __forceinline__ void hegv_block_body(const BlockProblem& pr) {
     extern __shared__ __align__(16) unsigned char sm[];
     double2* A = reinterpret_cast<double2*>(sm);
     double2* xw = A + (size_t)n * P + (size_t)warp * n;  // this warp's column
+    double2* part = A + (size_t)n * P;                     // the columns' area as one array
     unsigned char* vb = sm + region_a(n, nvec);
     double2* v = reinterpret_cast<double2*>(vb);
     vb += align16((size_t)n * 16);
@@ -152,7 +165,7 @@ __device__ __forceinline__ void hegv_block_body(const BlockProblem& pr) {
         if (tid == 0) *pr.info = n + *fail;
         return;
     }
-    inverse_to_global(n, P, A, wv, xw, Uinv);
+    inverse_to_global(n, P, A, wv, Uinv);
     __syncthreads();
 
     // ---- 3. C = U^{-H} H U^{-1}
@@ -284,12 +297,26 @@ __device__ __forceinline__ void hegv_block_body(const BlockProblem& pr) {
         __syncthreads();
         const double2 tk = tau[k];
         for (int r = tid; r < m; r += kBT) W2[(k + 1 + r) + (size_t)k * n] = v[r];
-        // p = tau C22 v, one warp per row
-        for (int r = warp; r < m; r += kBW) {
+        // p = tau C22 v: warp q sums columns q, q + kBW, ... of rows lane, lane + 32,
+        // ... into part[q][row] (the per-warp column area, unused here: kBW n >= kBW m);
+        // then one thread per row adds the kBW partial sums
+        for (int r = lane; r < m; r += 32) {
+            double2 s0 = mk(0.0, 0.0), s1 = mk(0.0, 0.0);
+            const double2* row = A + (k + 1 + r) + (size_t)(k + 1) * P;
+            int c = warp;
+            for (; c + kBW < m; c += 2 * kBW) {
+                cfma(s0, row[(size_t)c * P], v[c]);
+                cfma(s1, row[(size_t)(c + kBW) * P], v[c + kBW]);
+            }
+            if (c < m) cfma(s0, row[(size_t)c * P], v[c]);
+            part[warp * m + r] = s0 + s1;
+        }
+        __syncthreads();
+        if (tid < m) {
             double2 s = mk(0.0, 0.0);
-            for (int c = lane; c < m; c += 32) cfma(s, A[(k + 1 + r) + (size_t)(k + 1 + c) * P], v[c]);
-            s = wsum2(s);
-            if (lane == 0) pv[r] = cmul(tk, s);
+#pragma unroll
+            for (int q = 0; q < kBW; ++q) s = s + part[q * m + tid];
+            pv[tid] = cmul(tk, s);
         }
         __syncthreads();
         // alpha = -1/2 tau (p^H v), in every warp; w = p + alpha v; C22 -= v w^H + w v^H
@@ -297,11 +324,25 @@ __device__ __forceinline__ void hegv_block_body(const BlockProblem& pr) {
         for (int c = lane; c < m; c += 32) dot = dot + cmulc(pv[c], v[c]);
         dot = wsum2(dot);
         const double2 a2 = -0.5 * cmul(tk, dot);
-        for (int idx = tid; idx < m * m; idx += kBT) {
-            const int r = idx % m, c = idx / m;
-            const double2 wr = pv[r] + cmul(a2, v[r]), wc = pv[c] + cmul(a2, v[c]);
-            double2& x = A[(k + 1 + r) + (size_t)(k + 1 + c) * P];
-            x = x - cmulc(wc, v[r]) - cmulc(v[c], wr);
+        // C22 -= v w^H + w v^H: a warp per column, lanes along it; each lane keeps
+        // v and w of its rows in registers
+        {
+            double2 vr[kMaxRowsPerLane], wr[kMaxRowsPerLane];
+#pragma unroll
+            for (int q = 0; q < kMaxRowsPerLane; ++q) {
+                const int r = lane + 32 * q;
+                vr[q] = r < m ? v[r] : mk(0.0, 0.0);
+                wr[q] = r < m ? pv[r] + cmul(a2, vr[q]) : mk(0.0, 0.0);
+            }
+            for (int c = warp; c < m; c += kBW) {
+                const double2 vc = conj2(v[c]), wc = conj2(pv[c] + cmul(a2, v[c]));
+                double2* col = A + (k + 1) + (size_t)(k + 1 + c) * P;
+#pragma unroll
+                for (int q = 0; q < kMaxRowsPerLane; ++q) {
+                    const int r = lane + 32 * q;
+                    if (r < m) col[r] = col[r] - cmul(vr[q], wc) - cmul(wr[q], vc);
+                }
+            }
         }
         __syncthreads();
     }
@@ -331,32 +372,42 @@ __device__ __forceinline__ void hegv_block_body(const BlockProblem& pr) {
     }
     __syncthreads();
     {
-        constexpr int S = 2, NP = 32 * S;  // points per round
+        // eight lanes per eigenvalue, four eigenvalues a warp: a round counts at
+        // 16 interior points and keeps the seventeenth of the interval holding it
+        constexpr int G = 8, S = 2, NP = G * S;
+        const int grp = lane / G, sub = lane % G;
         const double scale = bounds[2];
         const double pivmin = fmax(1e-290, 1e-300 * scale * scale);
         const double tol = 4.0 * 2.220446049250313e-16 * fmax(scale, 1e-300);
-        for (int i = warp; i < nvec; i += kBW) {
+        for (int base = warp * (32 / G); base < nvec; base += kBW * (32 / G)) {
+            const int i = base + grp;
+            const bool valid = i < nvec;
             double a = bounds[0], bb = bounds[1];
-            for (int it = 0; it < 64 && (bb - a) > tol; ++it) {
+            for (int it = 0; it < 64; ++it) {
+                const bool active = valid && (bb - a) > tol;
+                if (!__any_sync(0xffffffffu, active)) break;
                 double x[S];
                 int cnt[S];
 #pragma unroll
-                for (int s = 0; s < S; ++s) x[s] = a + (bb - a) * (lane * S + s + 1) / (NP + 1.0);
+                for (int s = 0; s < S; ++s) x[s] = a + (bb - a) * (sub * S + s + 1) / (NP + 1.0);
                 sturm_counts<S>(n, d, e2, x, pivmin, cnt);
                 int first = S;
 #pragma unroll
                 for (int s = S - 1; s >= 0; --s)
                     if (cnt[s] > i) first = s;
-                const unsigned above = __ballot_sync(0xffffffffu, first < S);
-                const int l = above ? __ffs(above) - 1 : 32;
-                const int fl = __shfl_sync(0xffffffffu, first, l & 31);
-                const int mpt = (l == 32) ? NP : l * S + fl;
-                const double na = (mpt == 0) ? a : a + (bb - a) * mpt / (NP + 1.0);
-                const double nb = (mpt == NP) ? bb : a + (bb - a) * (mpt + 1) / (NP + 1.0);
-                a = na;
-                bb = nb;
+                const unsigned ball = __ballot_sync(0xffffffffu, first < S);
+                const unsigned gm = (ball >> (grp * G)) & ((1u << G) - 1u);
+                const int l = gm ? __ffs(gm) - 1 : G;
+                const int fl = __shfl_sync(0xffffffffu, first, grp * G + (l & (G - 1)));
+                if (active) {
+                    const int mpt = (l == G) ? NP : l * S + fl;
+                    const double na = (mpt == 0) ? a : a + (bb - a) * mpt / (NP + 1.0);
+                    const double nb = (mpt == NP) ? bb : a + (bb - a) * (mpt + 1) / (NP + 1.0);
+                    a = na;
+                    bb = nb;
+                }
             }
-            if (lane == 0) wv[i] = 0.5 * (a + bb);
+            if (valid && sub == 0) wv[i] = 0.5 * (a + bb);
         }
     }
     __syncthreads();
@@ -463,39 +514,57 @@ __device__ __forceinline__ void hegv_block_body(const BlockProblem& pr) {
         if (r > k + 1) A[r + (size_t)k * P] = W2[r + (size_t)k * n];
     }
     __syncthreads();
-    for (int c = warp; c < nvec; c += kBW) {
-        double2 z[kMaxRowsPerLane];
+    constexpr int kCols = 3;  // vectors a warp carries through the reflectors together
+    for (int c0 = warp; c0 < nvec; c0 += kCols * kBW) {
+        double2 z[kCols][kMaxRowsPerLane];
 #pragma unroll
-        for (int q = 0; q < kMaxRowsPerLane; ++q) {
-            const int r = lane + 32 * q;
-            z[q] = r < n ? Z[r + (size_t)c * n] : mk(0.0, 0.0);
+        for (int j = 0; j < kCols; ++j) {
+            const int c = c0 + j * kBW;
+#pragma unroll
+            for (int q = 0; q < kMaxRowsPerLane; ++q) {
+                const int r = lane + 32 * q;
+                z[j][q] = (c < nvec && r < n) ? Z[r + (size_t)c * n] : mk(0.0, 0.0);
+            }
         }
         // Q y = H_0 H_1 ... H_{n-2} y: the last reflector first
         for (int k = n - 2; k >= 0; --k) {
-            double2 s = mk(0.0, 0.0);
+            double2 vr[kMaxRowsPerLane];
 #pragma unroll
             for (int q = 0; q < kMaxRowsPerLane; ++q) {
                 const int r = lane + 32 * q;
-                if (r > k && r < n) {
-                    const double2 vr = r == k + 1 ? mk(1.0, 0.0) : A[r + (size_t)k * P];
-                    s = s + cmulc(vr, z[q]);
-                }
+                vr[q] = (r > k && r < n) ? (r == k + 1 ? mk(1.0, 0.0) : A[r + (size_t)k * P]) : mk(0.0, 0.0);
             }
-            s = wsum2(s);
-            const double2 ts = cmul(tau[k], s);
+            double2 s[kCols];
 #pragma unroll
-            for (int q = 0; q < kMaxRowsPerLane; ++q) {
-                const int r = lane + 32 * q;
-                if (r > k && r < n) {
-                    const double2 vr = r == k + 1 ? mk(1.0, 0.0) : A[r + (size_t)k * P];
-                    z[q] = z[q] - cmul(vr, ts);
+            for (int j = 0; j < kCols; ++j) {
+                s[j] = mk(0.0, 0.0);
+#pragma unroll
+                for (int q = 0; q < kMaxRowsPerLane; ++q) s[j] = s[j] + cmulc(vr[q], z[j][q]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int j = 0; j < kCols; ++j) {
+                    s[j].x += __shfl_xor_sync(0xffffffffu, s[j].x, o);
+                    s[j].y += __shfl_xor_sync(0xffffffffu, s[j].y, o);
                 }
+            const double2 tk = tau[k];
+#pragma unroll
+            for (int j = 0; j < kCols; ++j) {
+                const double2 ts = cmul(tk, s[j]);
+#pragma unroll
+                for (int q = 0; q < kMaxRowsPerLane; ++q) z[j][q] = z[j][q] - cmul(vr[q], ts);
             }
         }
 #pragma unroll
-        for (int q = 0; q < kMaxRowsPerLane; ++q) {
-            const int r = lane + 32 * q;
-            if (r < n) Z[r + (size_t)c * n] = z[q];
+        for (int j = 0; j < kCols; ++j) {
+            const int c = c0 + j * kBW;
+            if (c >= nvec) continue;
+#pragma unroll
+            for (int q = 0; q < kMaxRowsPerLane; ++q) {
+                const int r = lane + 32 * q;
+                if (r < n) Z[r + (size_t)c * n] = z[j][q];
+            }
         }
     }
     __syncthreads();
@@ -508,9 +577,16 @@ __device__ __forceinline__ void hegv_block_body(const BlockProblem& pr) {
         for (int r = lane; r < n; r += 32) xw[r] = Z[r + (size_t)c * n];
         __syncwarp();
         for (int r = lane; r < n; r += 32) {
-            double2 s = mk(0.0, 0.0);
-            for (int k = r; k < n; ++k) cfma(s, A[r + (size_t)k * P], xw[k]);
-            Z[r + (size_t)c * n] = s;
+            double2 s0 = mk(0.0, 0.0), s1 = mk(0.0, 0.0), s2 = mk(0.0, 0.0), s3 = mk(0.0, 0.0);
+            int k = r;
+            for (; k + 3 < n; k += 4) {
+                cfma(s0, A[r + (size_t)k * P], xw[k]);
+                cfma(s1, A[r + (size_t)(k + 1) * P], xw[k + 1]);
+                cfma(s2, A[r + (size_t)(k + 2) * P], xw[k + 2]);
+                cfma(s3, A[r + (size_t)(k + 3) * P], xw[k + 3]);
+            }
+            for (; k < n; ++k) cfma(s0, A[r + (size_t)k * P], xw[k]);
+            Z[r + (size_t)c * n] = (s0 + s1) + (s2 + s3);
         }
         __syncwarp();
     }
@@ -531,16 +607,15 @@ __global__ void __launch_bounds__(kBT, 1) hegv_block_many(const BlockProblem* ps
 __global__ void __launch_bounds__(kBT, 1)
 chol_inverse_block(int n, const double2* G, int ldg, double2* Uinv, int* info) {
     extern __shared__ __align__(16) unsigned char sm[];
-    const int P = pitch_of(n), warp = threadIdx.x >> 5;
+    const int P = pitch_of(n);
     double2* A = reinterpret_cast<double2*>(sm);
-    double2* xw = A + (size_t)n * P + (size_t)warp * n;
     double* rdiag = reinterpret_cast<double*>(sm + align16((size_t)n * P * 16 + (size_t)kBW * n * 16));
     int* fail = reinterpret_cast<int*>(rdiag + n);
     if (!cholesky_in_smem(n, P, G, ldg, A, rdiag, fail)) {
         if (threadIdx.x == 0) *info = *fail;
         return;
     }
-    inverse_to_global(n, P, A, rdiag, xw, Uinv);
+    inverse_to_global(n, P, A, rdiag, Uinv);
     if (threadIdx.x == 0) *info = 0;
 }
 

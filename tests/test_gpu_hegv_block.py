@@ -1,7 +1,7 @@
 """The one-block subspace eigensolver (q3_b200/csrc/dense_block.cu) on the GPU.
 
 Problems of order up to about 110 fit one thread block; the library solves
-them there alone up to order 56 (the Davidson's subspace solves of small
+them there alone up to order 64 (the Davidson's subspace solves of small
 cells) and many per launch at any fitting order (q3b_hegv_batched).  Checked
 against LAPACK (scipy's zhegv) and against the multi-kernel path of the same
 library: eigenvalues within 1e-12 of the largest |eigenvalue| (times n/16 above
