@@ -13,8 +13,9 @@
 //      shared copy of H, then U^{-H} T), kept Hermitian from its upper triangle;
 //   4. C = Q T Q^H, Householder reflectors H_k = I - tau_k v_k v_k^H chosen so
 //      that the subdiagonal comes out real (LAPACK's zlarfg convention), one
-//      column per step: the reflector by one warp, p = tau C v by a warp per
-//      row, the rank-2 update C -= v w^H + w v^H by all threads;
+//      column per step: p = tau C v by warp-column partial sums, the rank-2
+//      update C -= v w^H + w v^H a warp per column, and the next reflector by
+//      warp 0 from the first updated column while the others finish;
 //   5. the lowest nvec eigenvalues of the real tridiagonal by multisection on
 //      Sturm counts, one warp per eigenvalue;
 //   6. their eigenvectors by inverse iteration, one thread per cluster of close
@@ -51,7 +52,7 @@ __host__ __device__ inline size_t region_a(int n, int nvec) {
     return align16(mat > inv ? mat : inv);
 }
 __host__ __device__ inline size_t vec_bytes(int n) {
-    return 3 * align16((size_t)n * 16) + 4 * align16((size_t)n * 8) + 64;
+    return 4 * align16((size_t)n * 16) + 4 * align16((size_t)n * 8) + 64;
 }
 
 __device__ __forceinline__ double2 wsum2(double2 v) {
@@ -145,6 +146,8 @@ __device__ __forceinline__ void hegv_block_body(const BlockProblem& pr) {
     double2* pv = reinterpret_cast<double2*>(vb);
     vb += align16((size_t)n * 16);
     double2* tau = reinterpret_cast<double2*>(vb);
+    vb += align16((size_t)n * 16);
+    double2* v2 = reinterpret_cast<double2*>(vb);  // the other reflector buffer
     vb += align16((size_t)n * 16);
     double* d = reinterpret_cast<double*>(vb);
     vb += align16((size_t)n * 8);
@@ -261,42 +264,52 @@ __device__ __forceinline__ void hegv_block_body(const BlockProblem& pr) {
     __syncthreads();
 
     // ---- 4. Householder tridiagonalisation, reflectors to W2
+    // Warp 0 forms the reflector of column k (x = C[k+1:n, k]) into vk, with tau[k],
+    // d[k] and e[k].  From the second column on it does so inside the previous step:
+    // column k is the first column of that step's trailing update, which warp 0
+    // updates alone and then turns into the next reflector while the other warps
+    // update the rest (one phase and one barrier fewer per step).  v alternates
+    // between two buffers, as the other warps still read step k's.
+    auto reflector = [&](int k, double2* vk) {
+        const int m = n - k - 1;
+        double ss = 0.0;
+        for (int r = 1 + lane; r < m; r += 32) {
+            const double2 xr = A[(k + 1 + r) + (size_t)k * P];
+            ss += xr.x * xr.x + xr.y * xr.y;
+        }
+        ss = wsum1(ss);
+        const double2 al = A[(k + 1) + (size_t)k * P];
+        double2 tk, scal;
+        double beta;
+        if (ss == 0.0 && al.y == 0.0) {
+            tk = mk(0.0, 0.0);
+            scal = mk(0.0, 0.0);
+            beta = al.x;
+        } else {
+            const double nrm = sqrt(al.x * al.x + al.y * al.y + ss);
+            beta = al.x >= 0.0 ? -nrm : nrm;
+            tk = mk((beta - al.x) / beta, -al.y / beta);
+            // 1 / (alpha - beta)
+            const double2 den = mk(al.x - beta, al.y);
+            const double dd = 1.0 / (den.x * den.x + den.y * den.y);
+            scal = mk(den.x * dd, -den.y * dd);
+        }
+        for (int r = lane; r < m; r += 32)
+            vk[r] = r == 0 ? mk(1.0, 0.0) : cmul(A[(k + 1 + r) + (size_t)k * P], scal);
+        if (lane == 0) {
+            d[k] = A[k + (size_t)k * P].x;
+            e[k] = beta;
+            tau[k] = tk;
+        }
+    };
+    double2* vbuf[2] = {v, v2};
+    if (warp == 0 && n > 1) reflector(0, vbuf[0]);
+    __syncthreads();
     for (int k = 0; k + 1 < n; ++k) {
         const int m = n - k - 1;  // x = C[k+1:n, k]
-        if (warp == 0) {
-            double ss = 0.0;
-            for (int r = 1 + lane; r < m; r += 32) {
-                const double2 xr = A[(k + 1 + r) + (size_t)k * P];
-                ss += xr.x * xr.x + xr.y * xr.y;
-            }
-            ss = wsum1(ss);
-            const double2 al = A[(k + 1) + (size_t)k * P];
-            double2 tk, scal;
-            double beta;
-            if (ss == 0.0 && al.y == 0.0) {
-                tk = mk(0.0, 0.0);
-                scal = mk(0.0, 0.0);
-                beta = al.x;
-            } else {
-                const double nrm = sqrt(al.x * al.x + al.y * al.y + ss);
-                beta = al.x >= 0.0 ? -nrm : nrm;
-                tk = mk((beta - al.x) / beta, -al.y / beta);
-                // 1 / (alpha - beta)
-                const double2 den = mk(al.x - beta, al.y);
-                const double dd = 1.0 / (den.x * den.x + den.y * den.y);
-                scal = mk(den.x * dd, -den.y * dd);
-            }
-            for (int r = lane; r < m; r += 32)
-                v[r] = r == 0 ? mk(1.0, 0.0) : cmul(A[(k + 1 + r) + (size_t)k * P], scal);
-            if (lane == 0) {
-                d[k] = A[k + (size_t)k * P].x;
-                e[k] = beta;
-                tau[k] = tk;
-            }
-        }
-        __syncthreads();
+        const double2* vk = vbuf[k & 1];
         const double2 tk = tau[k];
-        for (int r = tid; r < m; r += kBT) W2[(k + 1 + r) + (size_t)k * n] = v[r];
+        for (int r = tid; r < m; r += kBT) W2[(k + 1 + r) + (size_t)k * n] = vk[r];
         // p = tau C22 v: warp q sums columns q, q + kBW, ... of rows lane, lane + 32,
         // ... into part[q][row] (the per-warp column area, unused here: kBW n >= kBW m);
         // then one thread per row adds the kBW partial sums
@@ -305,10 +318,10 @@ __device__ __forceinline__ void hegv_block_body(const BlockProblem& pr) {
             const double2* row = A + (k + 1 + r) + (size_t)(k + 1) * P;
             int c = warp;
             for (; c + kBW < m; c += 2 * kBW) {
-                cfma(s0, row[(size_t)c * P], v[c]);
-                cfma(s1, row[(size_t)(c + kBW) * P], v[c + kBW]);
+                cfma(s0, row[(size_t)c * P], vk[c]);
+                cfma(s1, row[(size_t)(c + kBW) * P], vk[c + kBW]);
             }
-            if (c < m) cfma(s0, row[(size_t)c * P], v[c]);
+            if (c < m) cfma(s0, row[(size_t)c * P], vk[c]);
             part[warp * m + r] = s0 + s1;
         }
         __syncthreads();
@@ -319,23 +332,24 @@ __device__ __forceinline__ void hegv_block_body(const BlockProblem& pr) {
             pv[tid] = cmul(tk, s);
         }
         __syncthreads();
-        // alpha = -1/2 tau (p^H v), in every warp; w = p + alpha v; C22 -= v w^H + w v^H
+        // alpha = -1/2 tau (p^H v), in every warp; w = p + alpha v; C22 -= v w^H + w v^H:
+        // a warp per column, lanes along it, each lane's v and w in registers; warp 0
+        // takes the first column and then forms the next reflector from it
         double2 dot = mk(0.0, 0.0);
-        for (int c = lane; c < m; c += 32) dot = dot + cmulc(pv[c], v[c]);
+        for (int c = lane; c < m; c += 32) dot = dot + cmulc(pv[c], vk[c]);
         dot = wsum2(dot);
         const double2 a2 = -0.5 * cmul(tk, dot);
-        // C22 -= v w^H + w v^H: a warp per column, lanes along it; each lane keeps
-        // v and w of its rows in registers
         {
             double2 vr[kMaxRowsPerLane], wr[kMaxRowsPerLane];
 #pragma unroll
             for (int q = 0; q < kMaxRowsPerLane; ++q) {
                 const int r = lane + 32 * q;
-                vr[q] = r < m ? v[r] : mk(0.0, 0.0);
+                vr[q] = r < m ? vk[r] : mk(0.0, 0.0);
                 wr[q] = r < m ? pv[r] + cmul(a2, vr[q]) : mk(0.0, 0.0);
             }
-            for (int c = warp; c < m; c += kBW) {
-                const double2 vc = conj2(v[c]), wc = conj2(pv[c] + cmul(a2, v[c]));
+            const int c0 = warp == 0 ? 0 : warp, cstep = warp == 0 ? m : kBW - 1;
+            for (int c = c0; c < m; c += cstep) {
+                const double2 vc = conj2(vk[c]), wc = conj2(pv[c] + cmul(a2, vk[c]));
                 double2* col = A + (k + 1) + (size_t)(k + 1 + c) * P;
 #pragma unroll
                 for (int q = 0; q < kMaxRowsPerLane; ++q) {
@@ -343,6 +357,10 @@ __device__ __forceinline__ void hegv_block_body(const BlockProblem& pr) {
                     if (r < m) col[r] = col[r] - cmul(vr[q], wc) - cmul(wr[q], vc);
                 }
             }
+        }
+        if (warp == 0 && k + 2 < n) {
+            __syncwarp();  // the lanes' updates of column k+1 are visible to the whole warp
+            reflector(k + 1, vbuf[(k + 1) & 1]);
         }
         __syncthreads();
     }
