@@ -72,6 +72,10 @@ def parse():
                     help="bands for --probe density (39: one stick chunk of the 80^3 cell in FP64)")
     ap.add_argument("--hegv-orders", default="16,32,64,96,128,192,256,384,512",
                     help="orders for --probe hegv, comma separated")
+    ap.add_argument("--hegv-lowest", action="store_true",
+                    help="--probe hegv: the lowest n/2 eigenpairs (the Davidson's use) instead of all")
+    ap.add_argument("--block-order", type=int, default=-1,
+                    help="--probe hegv: the largest order solved in one thread block (-1: the library's)")
     return ap.parse_args()
 
 
@@ -1031,6 +1035,8 @@ def run_hegv_probe(args):
     ap = PlanewaveHamiltonianApplicator()
     ap.update_potential(sy.v_r, sy.cell.grid)
     ap.prepare_system_kpoint(sy)
+    if args.block_order >= 0:
+        ap.lib.q3b_set_block_eigensolver_order(int(args.block_order))
     dev = torch.device("cuda", ap.ctx.device)
     out = {}
     for n in (int(v) for v in args.hegv_orders.split(",") if v):
@@ -1048,7 +1054,11 @@ def run_hegv_probe(args):
         for _ in range(5):
             t0 = time.perf_counter()
             with ap.ctx.ordered_with_torch():
-                rc = ap.lib.q3b_hegv(ap.h, n, H.data_ptr(), S.data_ptr(), n, w.data_ptr(), Z.data_ptr())
+                if args.hegv_lowest:
+                    rc = ap.lib.q3b_hegv_lowest(ap.h, n, H.data_ptr(), S.data_ptr(), n, max(1, n // 2),
+                                                w.data_ptr(), Z.data_ptr())
+                else:
+                    rc = ap.lib.q3b_hegv(ap.h, n, H.data_ptr(), S.data_ptr(), n, w.data_ptr(), Z.data_ptr())
             torch.cuda.synchronize(dev)
             ts.append(time.perf_counter() - t0)
             if rc != 0:
