@@ -153,7 +153,7 @@ cgemm_kernel(int M, int N, int K, cplx_t<R> alpha, const cplx_t<R>* __restrict__
 // banks): A as [k][m] (pitch 132) when op(A) = A, as [m][k] (pitch 9) when
 // op(A) = A^H; B as [n][k] (pitch 9).
 namespace big {
-constexpr int BM = 128, BN = 64, BK = 8, STAGES = 3, THREADS = 256;
+constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3, THREADS = 256;
 constexpr int KP = BK + 1;         // [m][k] and [n][k]
 template <int TM> struct Shape {   // BM = 16 TM rows of C per block
     static constexpr int bm = 16 * TM;
