@@ -38,6 +38,10 @@ constexpr double kEmptyRelax = 5.0;         // tolerances.hpp:65
 constexpr double kEmptyFloor = 1e-5;        // tolerances.hpp:66
 constexpr double kStallBelow = 1e-5;        // Ry: the FP32 phase may stop on a plateau below this
 constexpr int kFlatIterations = 4;          // FP32 phase: iterations without a new band-energy low
+// FP32 phase: the occupied Ritz values' sum fell by less than kCrawlRelative of the
+// sum of their magnitudes over the last kCrawlWindow iterations
+constexpr int kCrawlWindow = 16;
+constexpr double kCrawlRelative = 2e-6;
 
 inline int grid_for(long n) { return stride_grid(n, 16); }
 
@@ -661,6 +665,7 @@ template <typename R> class Davidson {
         const double empty_tol = std::max(kEmptyRelax * tol, kEmptyFloor);
         double low = 0.0;
         int since_low = 0;
+        std::vector<double> sums;  // the occupied Ritz values' sum, per iteration
         for (int it = 0; it < max_it; ++it) {                            // :498
             int info = 0;
             if (reuse_collapse_ && basis == nb_) {
@@ -696,8 +701,14 @@ template <typename R> class Davidson {
             res.unconverged = static_cast<int>(unconv.size());
             if (it != 0) history.push_back(maxchange);
             const size_t h = history.size();
-            double occ_sum = 0.0;
-            for (int b = 0; b < occupied; ++b) occ_sum += whost_[b];
+            double occ_sum = 0.0, occ_abs = 0.0;
+            for (int b = 0; b < occupied; ++b) {
+                occ_sum += whost_[b];
+                occ_abs += std::fabs(whost_[b]);
+            }
+            sums.push_back(occ_sum);
+            const bool crawling = sums.size() > (size_t)kCrawlWindow &&
+                                  sums[sums.size() - 1 - kCrawlWindow] - occ_sum < kCrawlRelative * occ_abs;
             if (it == 0 || occ_sum < low) {
                 low = occ_sum;
                 since_low = 0;
@@ -706,7 +717,7 @@ template <typename R> class Davidson {
             }
             const bool stalled = stagnate && ((h >= 4 && history[h - 1] < kStallBelow &&
                                                history[h - 1] > 0.5 * history[h - 4]) ||
-                                              since_low >= kFlatIterations);
+                                              since_low >= kFlatIterations || crawling);
             if (unconv.empty() && !stalled && resid_gate_ > 0.0) {
                 const std::vector<double> r = residual_norms(basis);
                 for (int b = 0; b < occupied; ++b)
