@@ -38,3 +38,20 @@ def test_local_bytes_per_application(cid, sticks, mb64, mb32):
         local = kb["sticks_backward"] + kb["planes"] + kb["planes_v"] + kb["sticks_forward"]
         assert local == sy.nbands * (2 * kp.npw * c + 4 * s * n3 * c) + n * r + kp.npw * r
         assert abs(local / 1e6 - mb) < 0.01 * mb
+
+
+def test_plane_flops_of_the_bench_cell():
+    # the plane pass against the FP32 pipe: 5 n log2 n per line over the 35 stick rows and all
+    # 80 columns of each of the 80 planes, both ways, plus the V product: 12.17 GFLOP per
+    # 256-band application of config 1
+    import numpy as np
+    bench = _bench()
+    sy = synthetic.config(1)
+    kp = sy.kpoints[0]
+    n1, n2, n3 = sy.cell.grid
+    rows = len(np.unique(np.asarray(kp.g_to_grid) // (n2 * n3)))
+    assert rows == 35
+    fl = bench.plane_flops(kp, sy.cell.grid, sy.nbands)
+    line = 5.0 * 80 * np.log2(80)
+    assert fl == pytest.approx(256 * 80 * (2 * 35 * line + 2 * 80 * line + 2 * 80 * 80), rel=1e-12)
+    assert abs(fl / 1e9 - 12.17) < 0.01
