@@ -7,8 +7,9 @@
 // arithmetic.  Here one block of 512 threads holds the problem in shared
 // memory and runs every step with block barriers only:
 //   1. S = U^H U, the upper Cholesky factor in place (right-looking, one
-//      pivot row per step);
-//   2. U^{-1} by back substitution, one warp per column, to global scratch;
+//      pivot row per step, a warp per column of the trailing update);
+//   2. U^{-1} by back substitution, one thread per column (kept in the
+//      factor's free lower triangle), to global scratch;
 //   3. C = U^{-H} H U^{-1} as two register-tiled products (H U^{-1} from the
 //      shared copy of H, then U^{-H} T), kept Hermitian from its upper triangle;
 //   4. C = Q T Q^H, Householder reflectors H_k = I - tau_k v_k v_k^H chosen so
@@ -17,11 +18,11 @@
 //      update C -= v w^H + w v^H a warp per column, and the next reflector by
 //      warp 0 from the first updated column while the others finish;
 //   5. the lowest nvec eigenvalues of the real tridiagonal by multisection on
-//      Sturm counts, one warp per eigenvalue;
+//      Sturm counts, eight lanes per eigenvalue;
 //   6. their eigenvectors by inverse iteration, one thread per cluster of close
 //      eigenvalues with Gram-Schmidt inside the cluster (as dense.cu);
-//   7. z = U^{-1} Q y: the reflectors applied to each vector by one warp (the
-//      vector in registers), then the triangular product.
+//   7. z = U^{-1} Q y: the reflectors applied to three vectors at a time by one
+//      warp (the vectors in registers), then the triangular product.
 // Only __syncthreads / __syncwarp synchronise; nothing waits on another block.
 #include <algorithm>
 #include <mutex>
